@@ -1,0 +1,665 @@
+// capi.cu -- the C ABI (include/dol_b200.h): argument checks, workspace
+// handling, error reporting, and the one-call pipelines.
+#include <float.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <mutex>
+#include <string>
+
+#include "dol_b200.h"
+#include "gen.cuh"
+#include "kernels.h"
+
+namespace dolk {
+int g_num_sms = 148;
+}
+
+using namespace dolk;
+
+namespace {
+
+thread_local std::string t_err;
+
+dol_status fail(dol_status s, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return s;
+}
+
+// Per-device state: SM count and a mapped host word that kernels with bounded
+// waits set when a wait gives up (read by dol_sync).
+struct DeviceState {
+    bool ready = false;
+    int sms = 0;
+    int* err_host = nullptr;
+    int* err_dev = nullptr;
+};
+constexpr int kMaxDevices = 64;
+DeviceState g_dev[kMaxDevices];
+std::mutex g_init_mu;
+
+dol_status device_state(DeviceState** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(DOL_ERR_UNSUPPORTED, "device index %d out of range", dev);
+    DeviceState& s = g_dev[dev];
+    if (!s.ready) {
+        std::lock_guard<std::mutex> lock(g_init_mu);
+        if (!s.ready) {
+            int sms = 0;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
+            e = cudaHostAlloc(&s.err_host, sizeof(int), cudaHostAllocMapped);
+            if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaHostAlloc: %s", cudaGetErrorString(e));
+            *s.err_host = 0;
+            e = cudaHostGetDevicePointer(&s.err_dev, s.err_host, 0);
+            if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
+            s.sms = sms;
+            s.ready = true;
+        }
+    }
+    g_num_sms = s.sms;
+    *out = &s;
+    return DOL_OK;
+}
+
+// A pointer the GPU can dereference: device, managed, or mapped host memory.
+dol_status check_dev_ptr(const void* p, const char* name)
+{
+    if (!p) return fail(DOL_ERR_INVALID_ARG, "%s is NULL", name);
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DOL_ERR_INVALID_ARG, "%s is not a device pointer (%s)", name, cudaGetErrorString(e));
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return DOL_OK;
+    if (a.type == cudaMemoryTypeHost && a.devicePointer == p) return DOL_OK;
+    return fail(DOL_ERR_INVALID_ARG, "%s is not device-accessible memory", name);
+}
+
+dol_status check_dims(int w, int h, int d)
+{
+    if (w < 1 || h < 1 || d < 1) return fail(DOL_ERR_INVALID_ARG, "dimensions must be >= 1 (got %d x %d x %d)", w, h, d);
+    if ((long long)w * h * d > (1LL << 40)) return fail(DOL_ERR_INVALID_ARG, "volume too large");
+    return DOL_OK;
+}
+
+dol_status check_cw(int cw)
+{
+    if (cw < 1 || cw > 64) return fail(DOL_ERR_INVALID_ARG, "cell width cw must be in [1, 64] (got %d)", cw);
+    return DOL_OK;
+}
+
+dol_status launched(const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return DOL_OK;
+}
+
+// Workspace: the caller's, or a stream-ordered allocation freed after the work.
+struct Workspace {
+    void* ptr = nullptr;
+    bool owned = false;
+    cudaStream_t st = nullptr;
+    ~Workspace()
+    {
+        if (owned && ptr) cudaFreeAsync(ptr, st);
+    }
+};
+
+dol_status get_workspace(Workspace& ws, void* user, size_t user_bytes, size_t need, cudaStream_t st)
+{
+    ws.st = st;
+    if (need == 0) return DOL_OK;
+    if (user) {
+        if (user_bytes < need)
+            return fail(DOL_ERR_INVALID_ARG, "workspace too small: %zu bytes given, %zu needed", user_bytes, need);
+        dol_status s = check_dev_ptr(user, "workspace");
+        if (s != DOL_OK) return s;
+        ws.ptr = user;
+        return DOL_OK;
+    }
+    cudaError_t e = cudaMallocAsync(&ws.ptr, need, st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DOL_ERR_NO_MEMORY, "workspace allocation of %zu bytes failed: %s", need, cudaGetErrorString(e));
+    }
+    ws.owned = true;
+    return DOL_OK;
+}
+
+inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+// widest row the single-CTA sweeps handle (8 cells per thread, 512 threads)
+constexpr int kMaxSweepWidth = 4096;
+
+dol_status check_sweep_width(int w)
+{
+    if (w > kMaxSweepWidth)
+        return fail(DOL_ERR_UNSUPPORTED, "row width %d exceeds the sweep kernels' limit of %d", w, kMaxSweepWidth);
+    return DOL_OK;
+}
+
+#define DOL_TRY(x)                          \
+    do {                                    \
+        dol_status _s = (x);                \
+        if (_s != DOL_OK) return _s;        \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int dol_version(void) { return DOL_B200_VERSION; }
+
+const char* dol_status_string(dol_status s)
+{
+    switch (s) {
+        case DOL_OK: return "ok";
+        case DOL_ERR_INVALID_ARG: return "invalid argument";
+        case DOL_ERR_CUDA: return "CUDA error";
+        case DOL_ERR_NO_MEMORY: return "out of device memory";
+        case DOL_ERR_TIMEOUT: return "device-side wait timed out";
+        case DOL_ERR_UNSUPPORTED: return "unsupported size or option";
+    }
+    return "unknown status";
+}
+
+const char* dol_last_error(void) { return t_err.c_str(); }
+
+dol_status dol_sync(void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    cudaError_t e = cudaStreamSynchronize(S(stream));
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaStreamSynchronize: %s", cudaGetErrorString(e));
+    if (*(volatile int*)ds->err_host) {
+        *(volatile int*)ds->err_host = 0;
+        return fail(DOL_ERR_TIMEOUT, "a bounded device-side wait gave up; results of that call are invalid");
+    }
+    return DOL_OK;
+}
+
+size_t dol_mask_words(int w, int h, int d)
+{
+    if (w < 1 || h < 1 || d < 1) return 0;
+    return (size_t)((w + 31) / 32) * h * d;
+}
+
+// ---- host test-mask generators (the reference's own LCG and shapes) ---------------
+
+void dol_add_points_2d(int w, int h, int n, uint32_t seed, uint32_t* mask)
+{
+    const int ws = (w + 31) / 32;
+    for (int i = 0; i < n; i++) {
+        seed = lcg_next(seed);
+        int x = lcg_scale(seed, w);
+        seed = lcg_next(seed);
+        int y = lcg_scale(seed, h);
+        mask[(size_t)y * ws + (x >> 5)] |= 1u << (x & 31);
+    }
+}
+
+void dol_add_points_3d(int w, int h, int d, int n, uint32_t seed, uint32_t* mask)
+{
+    const int ws = (w + 31) / 32;
+    for (int i = 0; i < n; i++) {
+        seed = lcg_next(seed);
+        int x = lcg_scale(seed, w);
+        seed = lcg_next(seed);
+        int y = lcg_scale(seed, h);
+        seed = lcg_next(seed);
+        int z = lcg_scale(seed, d);
+        mask[((size_t)z * h + y) * ws + (x >> 5)] |= 1u << (x & 31);
+    }
+}
+
+static void fill_cells(int ws, int x0, int x1, int y0, int y1, uint32_t* slice)
+{
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++) slice[(size_t)y * ws + (x >> 5)] |= 1u << (x & 31);
+}
+
+void dol_add_block_2d(int w, int h, int sides, uint32_t* mask)
+{
+    const int ws = (w + 31) / 32;
+    const int x0 = w / 4, x1 = x0 + w / 2 - 1, y0 = h / 3, y1 = y0 + h / 3 - 1;
+    if (sides > 4) { fill_cells(ws, x0, x1, y0, y1, mask); return; }
+    if (sides > 0) fill_cells(ws, x0, x1, y0, y0, mask);
+    if (sides > 1) fill_cells(ws, x0, x0, y0, y1, mask);
+    if (sides > 2) fill_cells(ws, x0, x1, y1, y1, mask);
+    if (sides > 3) fill_cells(ws, x1, x1, y0, y1, mask);
+}
+
+void dol_add_block_3d(int w, int h, int d, int sides, uint32_t* mask)
+{
+    const int ws = (w + 31) / 32;
+    const int x0 = w / 4, x1 = x0 + w / 2 - 1, y0 = h / 3, y1 = y0 + h / 3 - 1, z0 = d / 3, z1 = z0 + d / 3 - 1;
+    auto box = [&](int a0, int a1, int b0, int b1, int c0, int c1) {
+        for (int z = c0; z <= c1; z++) fill_cells(ws, a0, a1, b0, b1, mask + (size_t)z * ws * h);
+    };
+    if (sides > 6) { box(x0, x1, y0, y1, z0, z1); return; }
+    if (sides > 0) box(x0, x1, y0, y1, z0, z0);
+    if (sides > 1) box(x0, x0, y0, y1, z0, z1);
+    if (sides > 2) box(x0, x1, y0, y0, z0, z1);
+    if (sides > 3) box(x1, x1, y0, y1, z0, z1);
+    if (sides > 4) box(x0, x1, y1, y1, z0, z1);
+    if (sides > 5) box(x0, x1, y0, y1, z1, z1);
+}
+
+// ---- byte mask -> bitmask ---------------------------------------------------------------
+
+dol_status dol_pack_bytemask(int w, int h, int d, const uint8_t* bytes, int threshold, int less_than, uint32_t* mask,
+                             void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(bytes, "bytes"));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    launch_pack_bytemask(bytes, mask, w, (long long)h * d, threshold, less_than, S(stream));
+    return launched("pack_bytemask");
+}
+
+// ---- initialisation -------------------------------------------------------------------
+
+dol_status dol_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, float max_d, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    launch_init_distances(mask, dist, w, h, max_d, S(stream));
+    return launched("init_distances_2d");
+}
+
+dol_status dol_init_deltas_2d(int w, int h, const uint32_t* mask, dol_delta2* deltas, int invert, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_init_deltas(2, mask, deltas, w, h, invert, S(stream));
+    return launched("init_deltas_2d");
+}
+
+dol_status dol_init_deltas_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, int invert, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_init_deltas(3, mask, deltas, w, (long long)h * d, invert, S(stream));
+    return launched("init_deltas_3d");
+}
+
+dol_status dol_init_border_2d(int w, int h, const uint32_t* mask, dol_delta2* deltas, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_init_border(2, mask, deltas, w, h, 1, S(stream));
+    return launched("init_border_2d");
+}
+
+dol_status dol_init_border_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_init_border(3, mask, deltas, w, h, d, S(stream));
+    return launched("init_border_3d");
+}
+
+// ---- propagation -------------------------------------------------------------------------
+
+dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_sweep_width(w));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_danielsson(2, deltas, w, h, 1, cw, S(stream));
+    return launched("danielsson_2d");
+}
+
+dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_sweep_width(w));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_danielsson(3, deltas, w, h, d, cw, S(stream));
+    return launched("danielsson_3d");
+}
+
+dol_status dol_fastsweep_2d(int w, int h, dol_delta2* deltas, int cw, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_sweep_width(w));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    launch_fastsweep_2d(deltas, w, h, cw, S(stream));
+    return launched("fastsweep_2d");
+}
+
+size_t dol_fastsweep_3d_workspace_size(int w, int h, int d) { return fastsweep3_workspace_bytes(w, h, d); }
+
+dol_status dol_fastsweep_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* workspace, size_t workspace_bytes,
+                            void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_sweep_width(w));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, fastsweep3_workspace_bytes(w, h, d), S(stream)));
+    launch_fastsweep_3d(deltas, w, h, d, cw, ws.ptr, ds->err_dev, S(stream));
+    return launched("fastsweep_3d");
+}
+
+size_t dol_jumpflood_2d_workspace_size(int w, int h) { return (size_t)w * h * sizeof(dol_delta2); }
+size_t dol_jumpflood_3d_workspace_size(int w, int h, int d) { return (size_t)w * h * d * sizeof(dol_delta3); }
+
+dol_status dol_jumpflood_2d(int w, int h, dol_delta2* deltas, int cw, void* workspace, size_t workspace_bytes,
+                            void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_jumpflood_2d_workspace_size(w, h), S(stream)));
+    launch_jumpflood(2, deltas, ws.ptr, w, h, 1, cw, S(stream));
+    return launched("jumpflood_2d");
+}
+
+dol_status dol_jumpflood_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* workspace, size_t workspace_bytes,
+                            void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_jumpflood_3d_workspace_size(w, h, d), S(stream)));
+    launch_jumpflood(3, deltas, ws.ptr, w, h, d, cw, S(stream));
+    return launched("jumpflood_3d");
+}
+
+// ---- Felzenszwalb ----------------------------------------------------------------------------
+
+size_t dol_felzenszwalb_2d_workspace_size(int w, int h) { return felz_float_workspace_bytes(w, h); }
+
+dol_status dol_felzenszwalb_2d(int w, int h, float* dist, void* workspace, size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, felz_float_workspace_bytes(w, h), S(stream)));
+    launch_felz_float_2d(dist, w, h, ws.ptr, S(stream));
+    return launched("felzenszwalb_2d");
+}
+
+size_t dol_edt_mask_2d_workspace_size(int w, int h) { return edt_workspace_bytes(2, w, h, 1); }
+size_t dol_edt_mask_3d_workspace_size(int w, int h, int d) { return edt_workspace_bytes(3, w, h, d); }
+
+static dol_status edt_common(int dim, int w, int h, int d, const uint32_t* mask, float* out, int form, void* workspace,
+                             size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    if (form != DOL_EDT_SQUARED && form != DOL_EDT_DIST && form != DOL_EDT_SIGNED)
+        return fail(DOL_ERR_INVALID_ARG, "form must be DOL_EDT_SQUARED, DOL_EDT_DIST or DOL_EDT_SIGNED");
+    if (w > 32767 || h > 32767 || d > 32767) return fail(DOL_ERR_UNSUPPORTED, "EDT dimensions are limited to 32767");
+    if (h > 65535 || d > 65535) return fail(DOL_ERR_UNSUPPORTED, "EDT grid limit");
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(out, "out"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, edt_workspace_bytes(dim, w, h, d), S(stream)));
+    launch_edt_mask(dim, mask, out, w, h, d, form, ws.ptr, S(stream));
+    return launched("edt_mask");
+}
+
+dol_status dol_edt_mask_2d(int w, int h, const uint32_t* mask, float* out, int form, void* workspace,
+                           size_t workspace_bytes, void* stream)
+{
+    return edt_common(2, w, h, 1, mask, out, form, workspace, workspace_bytes, stream);
+}
+
+dol_status dol_edt_mask_3d(int w, int h, int d, const uint32_t* mask, float* out, int form, void* workspace,
+                           size_t workspace_bytes, void* stream)
+{
+    return edt_common(3, w, h, d, mask, out, form, workspace, workspace_bytes, stream);
+}
+
+// ---- deltas -> distances -------------------------------------------------------------------------
+
+dol_status dol_deltas_to_dist_2d(int w, int h, const dol_delta2* deltas, int cw, const uint32_t* sign_mask, float* out,
+                                 void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    DOL_TRY(check_dev_ptr(out, "out"));
+    if (sign_mask) DOL_TRY(check_dev_ptr(sign_mask, "sign_mask"));
+    launch_deltas_to_dist(2, deltas, cw, sign_mask, out, w, h, 1, S(stream));
+    return launched("deltas_to_dist_2d");
+}
+
+dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* deltas, int cw, const uint32_t* sign_mask,
+                                 float* out, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_cw(cw));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    DOL_TRY(check_dev_ptr(out, "out"));
+    if (sign_mask) DOL_TRY(check_dev_ptr(sign_mask, "sign_mask"));
+    launch_deltas_to_dist(3, deltas, cw, sign_mask, out, w, h, d, S(stream));
+    return launched("deltas_to_dist_3d");
+}
+
+// ---- one-call signed fields ----------------------------------------------------------------------
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t dol_sdf_workspace_size(int w, int h, int d, int method)
+{
+    const int dim = d > 1 ? 3 : 2;
+    const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
+    const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
+    if (method == DOL_FELZENSZWALB) return edt_workspace_bytes(dim, w, h, d);
+    size_t b = align256(cells * cb);                       // deltas, when the caller passes none
+    if (method == DOL_JUMPFLOOD) b += align256(cells * cb);  // ping-pong buffer
+    if (method == DOL_FASTSWEEP && dim == 3) b += align256(fastsweep3_workspace_bytes(w, h, d));
+    return b;
+}
+
+static dol_status sdf_common(int dim, int w, int h, int d, const uint32_t* mask, int method, void* deltas, float* dist,
+                             void* workspace, size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    if (deltas) DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    if (dist) DOL_TRY(check_dev_ptr(dist, "dist"));
+    if (!deltas && !dist) return fail(DOL_ERR_INVALID_ARG, "at least one of deltas / dist is required");
+    if (method != DOL_DANIELSSON && method != DOL_FASTSWEEP && method != DOL_JUMPFLOOD && method != DOL_FELZENSZWALB)
+        return fail(DOL_ERR_INVALID_ARG, "unknown method %d", method);
+    if (method == DOL_FELZENSZWALB && deltas)
+        return fail(DOL_ERR_INVALID_ARG, "Felzenszwalb produces distances only; pass deltas = NULL");
+    if (method == DOL_DANIELSSON || method == DOL_FASTSWEEP) DOL_TRY(check_sweep_width(w));
+    cudaStream_t st = S(stream);
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_sdf_workspace_size(w, h, dim == 3 ? d : 1, method), st));
+
+    if (method == DOL_FELZENSZWALB) {
+        launch_edt_mask(dim, mask, dist, w, h, d, DOL_EDT_SIGNED, ws.ptr, st);
+        return launched("sdf (felzenszwalb)");
+    }
+    const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
+    const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
+    char* p = static_cast<char*>(ws.ptr);
+    void* dl = deltas ? deltas : p;
+    p += align256(cells * cb);
+    launch_init_border(dim, mask, dl, w, h, d, st);
+    if (method == DOL_DANIELSSON) {
+        launch_danielsson(dim, dl, w, h, d, 2, st);
+    } else if (method == DOL_FASTSWEEP) {
+        if (dim == 2)
+            launch_fastsweep_2d(dl, w, h, 2, st);
+        else
+            launch_fastsweep_3d(dl, w, h, d, 2, p, ds->err_dev, st);
+    } else {
+        launch_jumpflood(dim, dl, p, w, h, d, 2, st);
+    }
+    if (dist) launch_deltas_to_dist(dim, dl, 2, mask, dist, w, h, d, st);
+    return launched("sdf");
+}
+
+dol_status dol_sdf_2d(int w, int h, const uint32_t* mask, int method, dol_delta2* deltas, float* dist, void* workspace,
+                      size_t workspace_bytes, void* stream)
+{
+    return sdf_common(2, w, h, 1, mask, method, deltas, dist, workspace, workspace_bytes, stream);
+}
+
+dol_status dol_sdf_3d(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* deltas, float* dist,
+                      void* workspace, size_t workspace_bytes, void* stream)
+{
+    return sdf_common(3, w, h, d, mask, method, deltas, dist, workspace, workspace_bytes, stream);
+}
+
+// ---- host-buffer variants --------------------------------------------------------------------------
+
+namespace {
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFreeAsync(p, st);
+    }
+    dol_status alloc(size_t n, cudaStream_t s)
+    {
+        st = s;
+        if (n == 0) return DOL_OK;
+        cudaError_t e = cudaMallocAsync(&p, n, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(DOL_ERR_NO_MEMORY, "device allocation of %zu bytes failed", n);
+        }
+        return DOL_OK;
+    }
+};
+
+struct OwnStream {
+    cudaStream_t st = nullptr;
+    ~OwnStream()
+    {
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+};
+
+dol_status copy(void* dst, const void* src, size_t n, cudaMemcpyKind k, cudaStream_t st)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, n, k, st);
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaMemcpyAsync: %s", cudaGetErrorString(e));
+    return DOL_OK;
+}
+}  // namespace
+
+static dol_status sdf_host(int dim, int w, int h, int d, const uint32_t* mask, int method, void* deltas, float* dist)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    if (!mask) return fail(DOL_ERR_INVALID_ARG, "mask is NULL");
+    if (!deltas && !dist) return fail(DOL_ERR_INVALID_ARG, "at least one of deltas / dist is required");
+    OwnStream os;
+    if (cudaStreamCreateWithFlags(&os.st, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(DOL_ERR_CUDA, "cudaStreamCreate failed");
+    const size_t cells = (size_t)w * h * d;
+    const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
+    const size_t mb = dol_mask_words(w, h, d) * sizeof(uint32_t);
+    DevBuf dm, dd, df;
+    DOL_TRY(dm.alloc(mb, os.st));
+    if (deltas) DOL_TRY(dd.alloc(cells * cb, os.st));
+    if (dist) DOL_TRY(df.alloc(cells * sizeof(float), os.st));
+    DOL_TRY(copy(dm.p, mask, mb, cudaMemcpyHostToDevice, os.st));
+    dol_status s = sdf_common(dim, w, h, d, static_cast<uint32_t*>(dm.p), method, dd.p, static_cast<float*>(df.p),
+                              nullptr, 0, os.st);
+    if (s != DOL_OK) return s;
+    if (deltas) DOL_TRY(copy(deltas, dd.p, cells * cb, cudaMemcpyDeviceToHost, os.st));
+    if (dist) DOL_TRY(copy(dist, df.p, cells * sizeof(float), cudaMemcpyDeviceToHost, os.st));
+    return dol_sync(os.st);
+}
+
+dol_status dol_sdf_2d_host(int w, int h, const uint32_t* mask, int method, dol_delta2* deltas, float* dist)
+{
+    return sdf_host(2, w, h, 1, mask, method, deltas, dist);
+}
+
+dol_status dol_sdf_3d_host(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* deltas, float* dist)
+{
+    return sdf_host(3, w, h, d, mask, method, deltas, dist);
+}
+
+dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float* out, int form)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    if (!mask || !out) return fail(DOL_ERR_INVALID_ARG, "mask and out are required");
+    OwnStream os;
+    if (cudaStreamCreateWithFlags(&os.st, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(DOL_ERR_CUDA, "cudaStreamCreate failed");
+    const size_t cells = (size_t)w * h * d;
+    const size_t mb = dol_mask_words(w, h, d) * sizeof(uint32_t);
+    DevBuf dm, df;
+    DOL_TRY(dm.alloc(mb, os.st));
+    DOL_TRY(df.alloc(cells * sizeof(float), os.st));
+    DOL_TRY(copy(dm.p, mask, mb, cudaMemcpyHostToDevice, os.st));
+    DOL_TRY(edt_common(3, w, h, d, static_cast<uint32_t*>(dm.p), static_cast<float*>(df.p), form, nullptr, 0, os.st));
+    DOL_TRY(copy(out, df.p, cells * sizeof(float), cudaMemcpyDeviceToHost, os.st));
+    return dol_sync(os.st);
+}
+
+}  // extern "C"

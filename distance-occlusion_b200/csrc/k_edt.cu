@@ -1,0 +1,353 @@
+// k_edt.cu -- exact Euclidean distance transform driven by a bitmask.
+//
+// The reference's Felzenszwalb transform (DistanceOcclusionLib.cpp:1026-1085,
+// driven by DistanceOcclusionTool.cpp:741-782) starts from 0 / FLT_MAX, so every
+// intermediate value is an integer squared distance below 2^24 and the float
+// envelope returns the exact squared EDT (FLT_MAX where no set cell exists);
+// any exact EDT gives identical floats.  This file computes it in integers,
+// separably, as three (2D: two) passes over the field:
+//
+//   x pass  from the mask bits: per cell, the distance along its row to the
+//           nearest cell of the opposite state, with the cell's own state in
+//           bit 15 (uint16).  One warp per row, word-level bit scans.
+//   y pass  per column: e(y) = min over y' of (y-y')^2 + f(y'), where f(y') is 0
+//           for cells of the opposite state and v(y')^2 otherwise.  The search
+//           walks outwards from y and stops once k^2 >= the best so far, which
+//           is exact because f >= 0.  Columns are staged in shared memory, 32
+//           adjacent x per CTA so global accesses are whole 64/128-byte rows.
+//   z pass  the same along z on the y-pass output (uint32, state in bit 31).
+//
+// Keeping "distance to the opposite state" per cell serves both forms at once:
+// for an empty cell it is the distance to the nearest set cell (the unsigned
+// EDT), for a set cell the distance to the nearest empty cell, so the signed
+// field (distance to set cells minus distance to empty cells) needs no second
+// transform.
+#include <float.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+#ifndef DOL_EDT_SQUARED
+#define DOL_EDT_SQUARED 0
+#define DOL_EDT_DIST 1
+#define DOL_EDT_SIGNED 2
+#endif
+
+namespace dolk {
+
+constexpr uint32_t kInf16 = 0x7FFFu;        // "no opposite cell in this row"
+constexpr uint32_t kInf32 = 0x7FFFFFFFu;    // "no opposite cell in this plane"
+constexpr int kMaxChunks = 32;              // rows up to 32*32*32 = 32768 cells
+
+// ---------------------------------------------------------------- x pass ----
+// One warp per row.  Per word: positions of its last / first clear and set
+// live bits; an exclusive prefix max (left) and suffix min (right) over the
+// words give the nearest cell of either state outside the word.
+__global__ void __launch_bounds__(256) k_edt_x(const uint32_t* __restrict__ mask, uint16_t* __restrict__ out, int w,
+                                               long long rows)
+{
+    __shared__ int right_carry[8][kMaxChunks][2];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int ws = words_per_row(w);
+    const int nchunks = (ws + 31) >> 5;
+    const int NEG = -(1 << 30), POS = 1 << 30;
+    long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+
+    for (long long row = warp; row < rows; row += nwarps) {
+        const uint32_t* mrow = mask + row * ws;
+        uint16_t* orow = out + row * (long long)w;
+
+        // right-to-left over chunks: first clear / set position right of each chunk
+        int carry0 = POS, carry1 = POS;
+        for (int c = nchunks - 1; c >= 0; c--) {
+            right_carry[wib][c][0] = carry0;
+            right_carry[wib][c][1] = carry1;
+            if (c == 0) break;
+            int k = 32 * c + lane;
+            int f0 = POS, f1 = POS;
+            if (k < ws) {
+                uint32_t live = live_bits(w, k), m = mrow[k];
+                uint32_t z0 = ~m & live, z1 = m & live;
+                if (z0) f0 = 32 * k + __ffs(z0) - 1;
+                if (z1) f1 = 32 * k + __ffs(z1) - 1;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                f0 = min(f0, __shfl_xor_sync(0xFFFFFFFFu, f0, o));
+                f1 = min(f1, __shfl_xor_sync(0xFFFFFFFFu, f1, o));
+            }
+            carry0 = min(carry0, f0);
+            carry1 = min(carry1, f1);
+        }
+        __syncwarp();
+
+        int left0 = NEG, left1 = NEG;   // last clear / set position left of the chunk
+        for (int c = 0; c < nchunks; c++) {
+            int k = 32 * c + lane;
+            uint32_t m = 0, live = 0;
+            int l0 = NEG, l1 = NEG, f0 = POS, f1 = POS;
+            if (k < ws) {
+                m = mrow[k];
+                live = live_bits(w, k);
+                uint32_t z0 = ~m & live, z1 = m & live;
+                if (z0) { l0 = 32 * k + 31 - __clz(z0); f0 = 32 * k + __ffs(z0) - 1; }
+                if (z1) { l1 = 32 * k + 31 - __clz(z1); f1 = 32 * k + __ffs(z1) - 1; }
+            }
+            // exclusive prefix max of last positions, exclusive suffix min of first positions
+            int p0 = l0, p1 = l1, s0 = f0, s1 = f1;
+            for (int o = 1; o < 32; o <<= 1) {
+                int a0 = __shfl_up_sync(0xFFFFFFFFu, p0, o), a1 = __shfl_up_sync(0xFFFFFFFFu, p1, o);
+                int b0 = __shfl_down_sync(0xFFFFFFFFu, s0, o), b1 = __shfl_down_sync(0xFFFFFFFFu, s1, o);
+                if (lane >= o) { p0 = max(p0, a0); p1 = max(p1, a1); }
+                if (lane + o < 32) { s0 = min(s0, b0); s1 = min(s1, b1); }
+            }
+            int ex0 = __shfl_up_sync(0xFFFFFFFFu, p0, 1), ex1 = __shfl_up_sync(0xFFFFFFFFu, p1, 1);
+            int ey0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1), ey1 = __shfl_down_sync(0xFFFFFFFFu, s1, 1);
+            if (lane == 0) { ex0 = NEG; ex1 = NEG; }
+            if (lane == 31) { ey0 = POS; ey1 = POS; }
+            ex0 = max(ex0, left0); ex1 = max(ex1, left1);
+            ey0 = min(ey0, right_carry[wib][c][0]); ey1 = min(ey1, right_carry[wib][c][1]);
+            // chunk totals feed the next chunk
+            int t0 = __shfl_sync(0xFFFFFFFFu, p0, 31), t1 = __shfl_sync(0xFFFFFFFFu, p1, 31);
+            left0 = max(left0, t0);
+            left1 = max(left1, t1);
+
+            // emit: word q of the chunk, lane = bit
+            for (int q = 0; q < 32; q++) {
+                int kq = 32 * c + q;
+                if (kq >= ws) break;
+                uint32_t mq = __shfl_sync(0xFFFFFFFFu, m, q), lq = __shfl_sync(0xFFFFFFFFu, live, q);
+                int L0 = __shfl_sync(0xFFFFFFFFu, ex0, q), L1 = __shfl_sync(0xFFFFFFFFu, ex1, q);
+                int R0 = __shfl_sync(0xFFFFFFFFu, ey0, q), R1 = __shfl_sync(0xFFFFFFFFu, ey1, q);
+                int x = 32 * kq + lane;
+                if (x < w) {
+                    int s = (mq >> lane) & 1u;
+                    uint32_t opp = (s ? ~mq : mq) & lq;          // cells of the other state in the word
+                    int Lo = s ? L0 : L1, Ro = s ? R0 : R1;      // ... and outside it
+                    uint32_t below = opp & ((1u << lane) - 1u);
+                    uint32_t above = lane == 31 ? 0u : (opp & ~((2u << lane) - 1u));
+                    int lpos = below ? 32 * kq + 31 - __clz(below) : Lo;
+                    int rpos = above ? 32 * kq + __ffs(above) - 1 : Ro;
+                    int dist = min(x - lpos, rpos - x);
+                    uint32_t v = dist >= (int)kInf16 ? kInf16 : (uint32_t)dist;
+                    orow[x] = (uint16_t)(v | ((uint32_t)s << 15));
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ line passes ----
+// A line runs along y (stride w) or z (stride w*h).  Each CTA owns 32 adjacent
+// x of one "outer" index and the whole line.  TIn is uint16 (x-pass output)
+// or uint32 (y-pass output).  kFinal writes the float field in the requested
+// form; otherwise uint32 (state << 31) | squared distance.
+
+template <typename TIn>
+__device__ __forceinline__ void decode_in(TIn v, uint32_t* state, uint32_t* f)
+{
+    if (sizeof(TIn) == 2) {
+        uint32_t u = (uint32_t)v;
+        *state = u >> 15;
+        uint32_t d = u & 0x7FFFu;
+        *f = d == kInf16 ? 0xFFFFFFFFu : d * d;
+    } else {
+        uint32_t u = (uint32_t)v;
+        *state = u >> 31;
+        uint32_t e = u & 0x7FFFFFFFu;
+        *f = e == kInf32 ? 0xFFFFFFFFu : e;
+    }
+}
+
+__device__ __forceinline__ float final_value(uint32_t state, uint32_t best, int form)
+{
+    // best == 0xFFFFFFFF: no cell of the other state anywhere on the lines searched
+    float e = best == 0xFFFFFFFFu ? FLT_MAX : (float)best;
+    if (form == DOL_EDT_SIGNED) {
+        float r = sqrtf(e);
+        return state ? -r : r;
+    }
+    if (state) return 0.0f;   // unsigned forms: set cells are at distance 0
+    return form == DOL_EDT_DIST ? sqrtf(e) : e;
+}
+
+template <typename TIn, bool kFinal, bool kStaged>
+__global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, void* __restrict__ out, int w, int n,
+                                                  long long stride, long long outer_stride, int form)
+{
+    extern __shared__ unsigned char smem_raw[];
+    TIn* tile = reinterpret_cast<TIn*>(smem_raw);   // [n][32]
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int x = blockIdx.x * 32 + lane;
+    const long long base = (long long)blockIdx.y * outer_stride + x;
+    const bool live = x < w;
+
+    if (kStaged) {
+        for (int q = wib; q < n; q += nw) tile[q * 32 + lane] = live ? in[base + q * stride] : (TIn)0;
+        __syncthreads();
+    }
+    auto at = [&](int q) -> TIn { return kStaged ? tile[q * 32 + lane] : in[base + q * stride]; };
+
+    for (int q = wib; q < n; q += nw) {
+        if (!live) continue;
+        uint32_t s, best;
+        decode_in<TIn>(at(q), &s, &best);
+        const int reach = max(q, n - 1 - q);
+        for (int k = 1; k <= reach; k++) {
+            uint32_t k2 = (uint32_t)k * (uint32_t)k;
+            if (k2 >= best) break;
+            if (q - k >= 0) {
+                uint32_t s2, f;
+                decode_in<TIn>(at(q - k), &s2, &f);
+                uint32_t c = s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2);
+                best = min(best, c);
+            }
+            if (q + k < n) {
+                uint32_t s2, f;
+                decode_in<TIn>(at(q + k), &s2, &f);
+                uint32_t c = s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2);
+                best = min(best, c);
+            }
+        }
+        long long o = base + q * stride;
+        if (kFinal) {
+            static_cast<float*>(out)[o] = final_value(s, best, form);
+        } else {
+            uint32_t e = best == 0xFFFFFFFFu ? kInf32 : best;
+            static_cast<uint32_t*>(out)[o] = e | (s << 31);
+        }
+    }
+}
+
+template <typename TIn, bool kFinal>
+static void line_pass(const TIn* in, void* out, int w, int n, long long stride, long long outer, long long outer_stride,
+                      int form, cudaStream_t st)
+{
+    size_t bytes = (size_t)n * 32 * sizeof(TIn);
+    const size_t kStageLimit = 200 * 1024;
+    dim3 grid((w + 31) / 32, (unsigned)outer);
+    const int threads = 256;
+    if (bytes <= kStageLimit) {
+        auto kern = k_edt_line<TIn, kFinal, true>;
+        if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        kern<<<grid, threads, bytes, st>>>(in, out, w, n, stride, outer_stride, form);
+    } else {
+        k_edt_line<TIn, kFinal, false><<<grid, threads, 0, st>>>(in, out, w, n, stride, outer_stride, form);
+    }
+}
+
+size_t edt_workspace_bytes(int dim, int w, int h, int d)
+{
+    size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
+    size_t b = cells * sizeof(uint16_t);
+    b = (b + 255) & ~(size_t)255;
+    if (dim == 3) b += cells * sizeof(uint32_t);
+    return b;
+}
+
+void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws,
+                     cudaStream_t st)
+{
+    long long rows = (long long)h * (dim == 3 ? d : 1);
+    size_t cells = (size_t)w * rows;
+    uint16_t* vx = static_cast<uint16_t*>(ws);
+    long long blocks = (rows * 32 + 255) / 256;
+    long long cap = (long long)g_num_sms * 16;
+    {
+        ProfScope ps("edt_x", st);
+        k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask, vx, w, rows);
+    }
+    if (dim == 2) {
+        ProfScope ps("edt_y_final", st);
+        line_pass<uint16_t, true>(vx, out, w, h, w, 1, 0, form, st);
+    } else {
+        size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
+        uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
+        long long plane = (long long)w * h;
+        {
+            ProfScope ps("edt_y", st);
+            line_pass<uint16_t, false>(vx, ey, w, h, w, d, plane, form, st);   // y lines, outer = z
+        }
+        ProfScope ps("edt_z_final", st);
+        line_pass<uint32_t, true>(ey, out, w, d, plane, h, w, form, st);   // z lines, outer = y
+    }
+}
+
+// ------------------------------------------------ faithful float Felzenszwalb ----
+// DOL::Felzenszwalb(w, h, float[]) on arbitrary input: the same 1D lower
+// envelope in the same float operations (DistanceOcclusionLib.cpp:1026-1062),
+// one thread per line.  Column pass into a scratch field, then row pass back.
+// Envelope stacks live in the workspace, interleaved by line for coalescing.
+
+__device__ void felz_line_dev(int n, const float* f, long long fstride, float* out, long long ostride, int* v, float* z,
+                              long long sstride)
+{
+    int k = 0;
+    v[0] = 0;
+    z[0] = -FLT_MAX;
+    z[sstride] = FLT_MAX;
+    for (int q = 1; q < n; q++) {
+        float hq = f[q * fstride] + (float)(q * q);
+        float s;
+        for (;;) {
+            int p = v[k * sstride];
+            float hp = f[p * fstride] + (float)(p * p);
+            s = __fdiv_rn(hq - hp, (float)(2 * (q - p)));
+            if (s > z[k * sstride]) break;
+            k--;
+        }
+        k++;
+        v[k * sstride] = q;
+        z[k * sstride] = s;
+        z[(k + 1) * sstride] = FLT_MAX;
+    }
+    k = 0;
+    for (int q = 0; q < n; q++) {
+        while (z[(k + 1) * sstride] < (float)q) k++;
+        int p = v[k * sstride];
+        out[q * ostride] = __fadd_rn((float)((q - p) * (q - p)), f[p * fstride]);
+    }
+}
+
+__global__ void k_felz_cols(const float* __restrict__ in, float* __restrict__ td, int w, int h, int* v, float* z)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= w) return;
+    // column x (stride w) -> td[x*h + q] (the reference's transposed scratch)
+    felz_line_dev(h, in + x, w, td + (long long)x * h, 1, v + x, z + x, w);
+}
+
+__global__ void k_felz_rows(const float* __restrict__ td, float* __restrict__ out, int w, int h, int* v, float* z)
+{
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= h) return;
+    felz_line_dev(w, td + y, h, out + (long long)y * w, 1, v + y, z + y, h);
+}
+
+size_t felz_float_workspace_bytes(int w, int h)
+{
+    size_t n = (size_t)(w > h ? w : h);
+    size_t lines = (size_t)(w > h ? w : h);
+    size_t td = ((size_t)w * h * sizeof(float) + 255) & ~(size_t)255;
+    size_t vb = (n * lines * sizeof(int) + 255) & ~(size_t)255;
+    size_t zb = (n + 1) * lines * sizeof(float);
+    return td + vb + zb;
+}
+
+void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st)
+{
+    size_t n = (size_t)(w > h ? w : h);
+    size_t lines = n;
+    char* p = static_cast<char*>(ws);
+    float* td = reinterpret_cast<float*>(p);
+    p += ((size_t)w * h * sizeof(float) + 255) & ~(size_t)255;
+    int* v = reinterpret_cast<int*>(p);
+    p += (n * lines * sizeof(int) + 255) & ~(size_t)255;
+    float* z = reinterpret_cast<float*>(p);
+    (void)lines;
+    // stacks are indexed [position * lines_in_pass + line]; each pass uses its own line count as the stride
+    k_felz_cols<<<(w + 127) / 128, 128, 0, st>>>(dist, td, w, h, v, z);
+    k_felz_rows<<<(h + 127) / 128, 128, 0, st>>>(td, dist, w, h, v, z);
+}
+
+}  // namespace dolk

@@ -1,0 +1,154 @@
+// k_jfa.cu -- JumpFlood passes and deltas -> distances.
+//
+// JumpFlood (DistanceOcclusionLib.cpp:782-908 for 2D, :2398-2472 for 3D) is a
+// ping-pong stencil: every cell of a pass reads only the previous pass, so one
+// thread per cell with the reference's fixed candidate order reproduces it
+// exactly.  The driver keeps the reference's pass schedule: steps from
+// FloorPow2(max dim - 1) halving to 1, plus one extra step-1 pass back into the
+// caller's buffer when the last result sits in the ping-pong buffer.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace dolk {
+
+__global__ void __launch_bounds__(256) k_jfa2(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int w,
+                                              int h, int s, int cw)
+{
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= w || y >= h) return;
+    const int o = cw * s;
+    auto at = [&](int xx, int yy) { return unpack2(__ldg(in + (long long)yy * w + xx)); };
+    C2 best = at(x, y);
+    // candidate order of :794-868
+    if (x - s >= 0) {
+        best = closer(best, add(at(x - s, y), -o, 0));
+        if (y - s >= 0) best = closer(best, add(at(x - s, y - s), -o, -o));
+        if (y + s < h) best = closer(best, add(at(x - s, y + s), -o, +o));
+    }
+    if (x + s < w) {
+        best = closer(best, add(at(x + s, y), +o, 0));
+        if (y - s >= 0) best = closer(best, add(at(x + s, y - s), +o, -o));
+        if (y + s < h) best = closer(best, add(at(x + s, y + s), +o, +o));
+    }
+    if (y - s >= 0) best = closer(best, add(at(x, y - s), 0, -o));
+    if (y + s < h) best = closer(best, add(at(x, y + s), 0, +o));
+    out[(long long)y * w + x] = pack2(best);
+}
+
+__device__ __forceinline__ C3 load3(const int16_t* p, long long i)
+{
+    const int16_t* c = p + 3 * i;
+    return C3{__ldg(c), __ldg(c + 1), __ldg(c + 2)};
+}
+__device__ __forceinline__ void store3(int16_t* p, long long i, C3 v)
+{
+    int16_t* c = p + 3 * i;
+    c[0] = (int16_t)v.x;
+    c[1] = (int16_t)v.y;
+    c[2] = (int16_t)v.z;
+}
+
+__global__ void __launch_bounds__(256) k_jfa3(const int16_t* __restrict__ in, int16_t* __restrict__ out, int w, int h,
+                                              int d, int s, int cw)
+{
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int z = blockIdx.z;
+    if (x >= w || y >= h) return;
+    const long long plane = (long long)w * h;
+    const long long idx = z * plane + (long long)y * w + x;
+    C3 best = load3(in, idx);
+    // all offsets in {-s, 0, +s}^3 that stay inside, z outermost, x innermost,
+    // skipping neighbours still at max (:2419-2438)
+    const int z0 = z - s >= 0 ? -s : 0, z1 = z + s < d ? s : 0;
+    const int y0 = y - s >= 0 ? -s : 0, y1 = y + s < h ? s : 0;
+    const int x0 = x - s >= 0 ? -s : 0, x1 = x + s < w ? s : 0;
+    for (int kz = z0; kz <= z1; kz += s)
+        for (int ky = y0; ky <= y1; ky += s)
+            for (int kx = x0; kx <= x1; kx += s) {
+                C3 c = load3(in, idx + kz * plane + (long long)ky * w + kx);
+                if (c.x == kMax3) continue;
+                best = closer(best, add(c, cw * kx, cw * ky, cw * kz));
+            }
+    store3(out, idx, best);
+}
+
+static int floor_pow2(int v)
+{
+    v |= v >> 1;
+    v |= v >> 2;
+    v |= v >> 4;
+    v |= v >> 8;
+    v |= v >> 16;
+    return (v + 1) >> 1;
+}
+
+void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, int cw, cudaStream_t st)
+{
+    int m = w > h ? w : h;
+    if (dim == 3 && d > m) m = d;
+    void* a = deltas;
+    void* b = temp;
+    auto pass = [&](int s, const void* src, void* dst) {
+        ProfScope ps("jumpflood_pass", st);
+        if (dim == 2) {
+            dim3 grid((w + 31) / 32, (h + 7) / 8);
+            k_jfa2<<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), w, h, s, cw);
+        } else {
+            dim3 grid((w + 31) / 32, (h + 7) / 8, d);
+            k_jfa3<<<grid, 256, 0, st>>>(static_cast<const int16_t*>(src), static_cast<int16_t*>(dst), w, h, d, s, cw);
+        }
+    };
+    for (int s = floor_pow2(m - 1); s > 0; s /= 2) {
+        pass(s, a, b);
+        void* t = a;
+        a = b;
+        b = t;
+    }
+    if (a != deltas) pass(1, a, deltas);
+}
+
+// ---- deltas -> distances (DistanceOcclusionTool.cpp:46-61, sign :1262/:1392) ----
+
+template <int kDim>
+__global__ void __launch_bounds__(256) k_deltas_to_dist(const void* __restrict__ deltas, int cw,
+                                                        const uint32_t* __restrict__ sign_mask, float* __restrict__ out,
+                                                        int w, long long rows)
+{
+    const int ws = words_per_row(w);
+    const long long n = rows * w;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int32_t l;
+        if (kDim == 2) {
+            l = len(unpack2(__ldg(static_cast<const uint32_t*>(deltas) + i)));
+        } else {
+            l = len(load3(static_cast<const int16_t*>(deltas), i));
+        }
+        float r = sqrtf((float)l);
+        if (cw != 1) r = __fdiv_rn(r, (float)cw);
+        if (sign_mask) {
+            long long row = i / w;
+            int x = (int)(i - row * w);
+            if ((__ldg(sign_mask + row * ws + (x >> 5)) >> (x & 31)) & 1u) r = -r;
+        }
+        out[i] = r;
+    }
+}
+
+void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* sign_mask, float* out, int w, int h,
+                           int d, cudaStream_t st)
+{
+    long long rows = (long long)h * (dim == 3 ? d : 1);
+    long long n = rows * w;
+    long long blocks = (n + 255) / 256;
+    long long cap = (long long)g_num_sms * 32;
+    int grid = (int)(blocks < cap ? blocks : cap);
+    ProfScope ps("deltas_to_dist", st);
+    if (dim == 2)
+        k_deltas_to_dist<2><<<grid, 256, 0, st>>>(deltas, cw, sign_mask, out, w, rows);
+    else
+        k_deltas_to_dist<3><<<grid, 256, 0, st>>>(deltas, cw, sign_mask, out, w, rows);
+}
+
+}  // namespace dolk

@@ -1,0 +1,400 @@
+// k_sweep.cu -- Danielsson and FastSweep, exact.
+//
+// Danielsson (DistanceOcclusionLib.cpp:702-778 2D, :2264-2394 3D) and FastSweep
+// 2D (:633-697) are serial in the sweep axis: every row needs the whole
+// previous row.  One CTA walks the rows of an image (or the slices and rows of
+// a volume); each thread keeps S consecutive cells of the current and previous
+// row in registers, so the vertical (and z) pulls are thread-local and only the
+// x passes talk across threads (row_pass in scan.cuh, exact).  The next row is
+// loaded while the current one is scanned.
+//
+// FastSweep 3D (:2186-2260) has more parallelism: row (y, z) of an octant
+// sweep needs only row (y-1, z) and row (y, z-1) of the same sweep, so rows on
+// an anti-diagonal y+z = c are independent.  k_fastsweep3 runs one octant per
+// launch with persistent CTAs that claim rows in anti-diagonal order from an
+// atomic counter and wait (bounded) on per-row ready flags.  A row is only
+// claimed by a running CTA and every row it waits on was claimed earlier, so
+// the earliest unfinished row can always proceed.
+#include "kernels.h"
+#include "scan.cuh"
+
+namespace dolk {
+
+// ---------------------------------------------------------------- helpers ----
+
+template <class Cell, int S, class P>
+__device__ __forceinline__ void load_row(Cell (&dst)[S], const P* base, long long row_first, int n)
+{
+#pragma unroll
+    for (int s = 0; s < S; s++)
+        if (s < n) dst[s] = cell_load(base, row_first + s);
+}
+template <class Cell, int S, class P>
+__device__ __forceinline__ void store_row(P* base, long long row_first, const Cell (&src)[S], int n)
+{
+#pragma unroll
+    for (int s = 0; s < S; s++)
+        if (s < n) cell_store(base, row_first + s, src[s]);
+}
+// L2-coherent loads for rows written by other CTAs of the same launch
+__device__ __forceinline__ C3 cell_load_cg(const int16_t* p, long long i)
+{
+    const int16_t* c = p + 3 * i;
+    return C3{__ldcg(c), __ldcg(c + 1), __ldcg(c + 2)};
+}
+
+// ------------------------------------------------------------ Danielsson 2D ----
+
+template <int S>
+__global__ void __launch_bounds__(512) k_danielsson2(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    __shared__ ScanShared<C2> sh;
+    const int t = threadIdx.x;
+    const int nseg = (w + S - 1) / S;
+    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const long long x0 = (long long)t * S;
+    C2 P[S], C[S], Cn[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = Cn[s] = V[s] = R[s] = D[s] = C2{0, 0};
+
+    // down sweep, rows 1..h-1 (:709-741)
+    load_row<C2, S>(P, dl, x0, n);
+    if (h > 1) load_row<C2, S>(C, dl, (long long)w + x0, n);
+    for (int y = 1; y < h; y++) {
+        if (y + 1 < h) load_row<C2, S>(Cn, dl, (long long)(y + 1) * w + x0, n);
+#pragma unroll
+        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, -cw));
+        row_pass<C2, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+        row_pass<C2, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
+        store_row<C2, S>(dl, (long long)y * w + x0, P, n);
+#pragma unroll
+        for (int s = 0; s < S; s++) C[s] = Cn[s];
+    }
+    // up sweep, rows h-2..0 (:745-777); P holds row h-1
+    if (h > 1) load_row<C2, S>(C, dl, (long long)(h - 2) * w + x0, n);
+    for (int y = h - 2; y >= 0; y--) {
+        if (y >= 1) load_row<C2, S>(Cn, dl, (long long)(y - 1) * w + x0, n);
+#pragma unroll
+        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, +cw));
+        row_pass<C2, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+        row_pass<C2, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
+        store_row<C2, S>(dl, (long long)y * w + x0, P, n);
+#pragma unroll
+        for (int s = 0; s < S; s++) C[s] = Cn[s];
+    }
+}
+
+// ------------------------------------------------------------ Danielsson 3D ----
+// Slices 1..d-1 then d-2..0 (:2355-2393); each slice takes the neighbouring
+// slice's cell with the z offset, then runs the 2D sweeps over its rows
+// (:2264-2345).  The z pull is folded into the first load of each row.
+
+template <int S>
+__global__ void __launch_bounds__(512) k_danielsson3(int16_t* __restrict__ dl, int w, int h, int d, int cw)
+{
+    __shared__ ScanShared<C3> sh;
+    const int t = threadIdx.x;
+    const int nseg = (w + S - 1) / S;
+    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const long long x0 = (long long)t * S;
+    const long long plane = (long long)w * h;
+    C3 P[S], C[S], Q[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = Q[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
+
+    for (int pass = 0; pass < 2; pass++) {
+        const int dz = pass == 0 ? -cw : +cw;
+        for (int k = 1; k < d; k++) {
+            const int z = pass == 0 ? k : d - 1 - k;
+            const int zp = pass == 0 ? z - 1 : z + 1;
+            const long long sb = z * plane, pb = (long long)zp * plane;
+            // row 0: z pull only
+            load_row<C3, S>(C, dl, sb + x0, n);
+            load_row<C3, S>(Q, dl, pb + x0, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) P[s] = closer(C[s], add(Q[s], 0, 0, dz));
+            store_row<C3, S>(dl, sb + x0, P, n);
+            // down sweep
+            for (int y = 1; y < h; y++) {
+                const long long rb = sb + (long long)y * w + x0;
+                load_row<C3, S>(C, dl, rb, n);
+                load_row<C3, S>(Q, dl, pb + (long long)y * w + x0, n);
+#pragma unroll
+                for (int s = 0; s < S; s++) V[s] = closer(closer(C[s], add(Q[s], 0, 0, dz)), add(P[s], 0, -cw, 0));
+                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+                row_pass<C3, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
+                store_row<C3, S>(dl, rb, P, n);
+            }
+            // up sweep
+            for (int y = h - 2; y >= 0; y--) {
+                const long long rb = sb + (long long)y * w + x0;
+                load_row<C3, S>(C, dl, rb, n);
+#pragma unroll
+                for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, +cw, 0));
+                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+                row_pass<C3, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
+                store_row<C3, S>(dl, rb, P, n);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- FastSweep 2D ----
+// Four quadrant sweeps; the first row of each sweep is left as is; each later
+// row takes the previous row's cell, then along x the previous cell of the row
+// and the diagonal cell of the previous row, in that order (:655-693).  The
+// previous row is also kept in shared memory for the diagonal candidates that
+// cross a segment boundary.
+
+template <int S>
+__global__ void __launch_bounds__(512) k_fastsweep2(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    __shared__ ScanShared<C2> sh;
+    extern __shared__ uint32_t prow[];   // [2][w]
+    const int t = threadIdx.x;
+    const int nseg = (w + S - 1) / S;
+    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const long long x0 = (long long)t * S;
+    C2 P[S], C[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = V[s] = R[s] = D[s] = C2{0, 0};
+
+    for (int sweep = 0; sweep < 4; sweep++) {
+        const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1;
+        const int ox = -cw * dx, oy = -cw * dy;
+        const int y0 = dy > 0 ? 0 : h - 1;
+        int buf = 0;
+        load_row<C2, S>(P, dl, (long long)y0 * w + x0, n);
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            if (s < n) prow[buf * w + x0 + s] = pack2(P[s]);
+        __syncthreads();
+        for (int j = 1; j < h; j++) {
+            const int y = y0 + j * dy;
+            load_row<C2, S>(C, dl, (long long)y * w + x0, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) {
+                V[s] = closer(C[s], add(P[s], 0, oy));
+                const long long xp = x0 + s - dx;
+                if (s < n && xp >= 0 && xp < w) D[s] = add(unpack2(prow[buf * w + xp]), ox, oy);
+            }
+            if (dx > 0)
+                row_pass<C2, S, true, +1>(R, V, t, nseg, n, cw, sh, D, false);
+            else
+                row_pass<C2, S, true, -1>(R, V, t, nseg, n, cw, sh, D, false);
+            store_row<C2, S>(dl, (long long)y * w + x0, R, n);
+            buf ^= 1;
+#pragma unroll
+            for (int s = 0; s < S; s++) {
+                P[s] = R[s];
+                if (s < n) prow[buf * w + x0 + s] = pack2(R[s]);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------- FastSweep 3D ----
+
+template <int S>
+__global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, int w, int h, int d, int cw, int sweep,
+                                                    int* __restrict__ flags, int* __restrict__ counter,
+                                                    const int* __restrict__ diag_start, int* __restrict__ err,
+                                                    int epoch)
+{
+    __shared__ ScanShared<C3> sh;
+    __shared__ int s_item;
+    const int t = threadIdx.x;
+    const int nseg = (w + S - 1) / S;
+    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const long long x0 = (long long)t * S;
+    const long long plane = (long long)w * h;
+    const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1, dz = (sweep & 4) ? -1 : 1;
+    const int oy = -cw * dy, oz = -cw * dz;
+    const int yb = dy > 0 ? 0 : h - 1, zb = dz > 0 ? 0 : d - 1;
+    const int H = h - 1, Dd = d - 1;
+    const long long total = (long long)H * Dd;
+    C3 C[S], Zp[S], Yp[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) C[s] = Zp[s] = Yp[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
+
+    for (;;) {
+        if (t == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        // anti-diagonal c = jj + kk (jj: rows after the first, kk: slices after the first)
+        int lo = 2, hi = H + Dd;
+        while (lo < hi) {   // last c with diag_start[c] <= item
+            int mid = (lo + hi + 1) >> 1;
+            if (diag_start[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        const int c = lo;
+        const int jj = max(1, c - Dd) + (int)(item - diag_start[c]);
+        const int kk = c - jj;
+        const int y = yb + jj * dy, z = zb + kk * dz;
+        const int yprev = y - dy, zprev = z - dz;
+
+        if (t == 0) {
+            // wait (bounded) until both neighbour rows of this sweep are done
+            const int* fa = jj > 1 ? flags + (long long)z * h + yprev : nullptr;
+            const int* fb = kk > 1 ? flags + (long long)zprev * h + y : nullptr;
+            for (int it = 0;; it++) {
+                bool ok = (!fa || *((volatile const int*)fa) >= epoch) && (!fb || *((volatile const int*)fb) >= epoch);
+                if (ok) break;
+                if (it > (1 << 22)) { atomicExch(err, 1); break; }
+                __nanosleep(128);
+            }
+            __threadfence();
+        }
+        __syncthreads();
+
+        const long long rb = z * plane + (long long)y * w + x0;
+        const long long zb_ = (long long)zprev * plane + (long long)y * w + x0;
+        const long long yb_ = z * plane + (long long)yprev * w + x0;
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            if (s < n) {
+                C[s] = cell_load_cg(dl, rb + s);
+                Zp[s] = cell_load_cg(dl, zb_ + s);
+                Yp[s] = cell_load_cg(dl, yb_ + s);
+                V[s] = closer(closer(C[s], add(Zp[s], 0, 0, oz)), add(Yp[s], 0, oy, 0));
+            }
+        if (dx > 0)
+            row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+        else
+            row_pass<C3, S, false, -1>(R, V, t, nseg, n, cw, sh, D, false);
+        store_row<C3, S>(dl, rb, R, n);
+        __threadfence();
+        __syncthreads();
+        if (t == 0) atomicExch(flags + (long long)z * h + y, epoch);
+    }
+}
+
+// --------------------------------------------------------------- launchers ----
+
+static int pick_s(int w, int max_threads)
+{
+    const int options[] = {1, 2, 4, 8};
+    for (int s : options)
+        if ((w + s - 1) / s <= max_threads && ((w + s - 1) / s > 64 || s == 1 || w <= 64 * s)) return s;
+    return (w + 7) / 8 <= max_threads ? 8 : 0;
+}
+
+static int threads_for(int w, int s)
+{
+    int n = (w + s - 1) / s;
+    return ((n + 31) / 32) * 32;
+}
+
+void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st)
+{
+    const int s = pick_s(w, 512);
+    const int T = threads_for(w, s);
+    ProfScope ps("danielsson", st);
+#define DOL_DAN_CASE(SV)                                                                              \
+    case SV:                                                                                          \
+        if (dim == 2)                                                                                 \
+            k_danielsson2<SV><<<1, T, 0, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);            \
+        else                                                                                          \
+            k_danielsson3<SV><<<1, T, 0, st>>>(static_cast<int16_t*>(deltas), w, h, d, cw);          \
+        break;
+    switch (s) {
+        DOL_DAN_CASE(1)
+        DOL_DAN_CASE(2)
+        DOL_DAN_CASE(4)
+        DOL_DAN_CASE(8)
+        default: break;
+    }
+#undef DOL_DAN_CASE
+}
+
+void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st)
+{
+    const int s = pick_s(w, 512);
+    const int T = threads_for(w, s);
+    const size_t smem = 2 * (size_t)w * sizeof(uint32_t);
+    ProfScope ps("fastsweep_2d", st);
+#define DOL_FS_CASE(SV)                                                                                      \
+    case SV: {                                                                                               \
+        auto kern = k_fastsweep2<SV>;                                                                        \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                 \
+        kern<<<1, T, smem, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);                                  \
+    } break;
+    switch (s) {
+        DOL_FS_CASE(1)
+        DOL_FS_CASE(2)
+        DOL_FS_CASE(4)
+        DOL_FS_CASE(8)
+        default: break;
+    }
+#undef DOL_FS_CASE
+}
+
+size_t fastsweep3_workspace_bytes(int w, int h, int d)
+{
+    (void)w;
+    size_t flags = (size_t)h * d * sizeof(int);
+    size_t diag = (size_t)(h + d + 2) * sizeof(int);
+    return ((flags + 255) & ~(size_t)255) + ((diag + 255) & ~(size_t)255) + 256;
+}
+
+void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, int* err, cudaStream_t st)
+{
+    if (h < 2 || d < 2) return;   // no row is ever updated (:2208, :2214 start at 1)
+    char* p = static_cast<char*>(ws);
+    int* flags = reinterpret_cast<int*>(p);
+    p += (((size_t)h * d * sizeof(int)) + 255) & ~(size_t)255;
+    int* diag = reinterpret_cast<int*>(p);
+    p += (((size_t)(h + d + 2) * sizeof(int)) + 255) & ~(size_t)255;
+    int* counters = reinterpret_cast<int*>(p);   // 8 ints
+
+    // anti-diagonal starts: rows jj in [1, h-1], kk in [1, d-1], c = jj + kk
+    const int H = h - 1, Dd = d - 1;
+    static thread_local int* host_diag = nullptr;
+    static thread_local size_t host_diag_n = 0;
+    size_t nd = (size_t)(H + Dd + 2);
+    if (host_diag_n < nd) {
+        if (host_diag) cudaFreeHost(host_diag);
+        cudaMallocHost(&host_diag, nd * sizeof(int));
+        host_diag_n = nd;
+    }
+    long long acc = 0;
+    for (int c = 0; c < (int)nd; c++) {
+        host_diag[c] = (int)acc;
+        if (c >= 2 && c <= H + Dd) {
+            int lo = c - Dd > 1 ? c - Dd : 1, hi = c - 1 < H ? c - 1 : H;
+            if (hi >= lo) acc += hi - lo + 1;
+        }
+    }
+    cudaMemcpyAsync(diag, host_diag, nd * sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(flags, 0, (size_t)h * d * sizeof(int), st);
+    cudaMemsetAsync(counters, 0, 8 * sizeof(int), st);
+
+    const int s = pick_s(w, 256);
+    const int T = threads_for(w, s);
+    ProfScope ps("fastsweep_3d", st);
+#define DOL_FS3_CASE(SV)                                                                                     \
+    case SV: {                                                                                               \
+        int per_sm = 0;                                                                                      \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fastsweep3<SV>, T, 0);                      \
+        if (per_sm < 1) per_sm = 1;                                                                          \
+        long long rows = (long long)H * Dd;                                                                  \
+        long long grid = (long long)per_sm * g_num_sms;                                                      \
+        if (grid > rows) grid = rows;                                                                        \
+        for (int sw = 0; sw < 8; sw++)                                                                       \
+            k_fastsweep3<SV><<<(int)grid, T, 0, st>>>(static_cast<int16_t*>(deltas), w, h, d, cw, sw, flags,  \
+                                                      counters + sw, diag, err, sw + 1);                     \
+    } break;
+    switch (s) {
+        DOL_FS3_CASE(1)
+        DOL_FS3_CASE(2)
+        DOL_FS3_CASE(4)
+        DOL_FS3_CASE(8)
+        default: break;
+    }
+#undef DOL_FS3_CASE
+}
+
+}  // namespace dolk

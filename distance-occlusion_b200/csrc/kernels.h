@@ -1,0 +1,59 @@
+// kernels.h -- launchers shared between the kernel files and the C ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+namespace dolk {
+
+extern int g_num_sms;   // set once per process by the C ABI layer
+
+// Brackets the launches in its scope with events on `st` when profiling is on
+// (dol_profile_begin / dol_profile_end); costs one mutex check otherwise.
+class ProfScope {
+public:
+    ProfScope(const char* name, cudaStream_t st);
+    ~ProfScope();
+
+private:
+    cudaStream_t st_;
+    int idx_ = -1;
+};
+
+inline uint32_t float_bits(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+// k_init.cu
+void launch_pack_bytemask(const uint8_t* bytes, uint32_t* mask, int w, long long rows, int threshold, int less_than,
+                          cudaStream_t st);
+void launch_init_distances(const uint32_t* mask, float* dist, int w, long long rows, float max_d, cudaStream_t st);
+void launch_init_deltas(int dim, const uint32_t* mask, void* deltas, int w, long long rows, int invert,
+                        cudaStream_t st);
+void launch_init_border(int dim, const uint32_t* mask, void* deltas, int w, int h, int d, cudaStream_t st);
+
+// k_edt.cu -- mask-driven exact EDT
+size_t edt_workspace_bytes(int dim, int w, int h, int d);
+void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws,
+                     cudaStream_t st);
+// faithful float Felzenszwalb (2D, arbitrary input)
+size_t felz_float_workspace_bytes(int w, int h);
+void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st);
+
+// k_jfa.cu
+void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, int cw, cudaStream_t st);
+void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* sign_mask, float* out, int w, int h,
+                           int d, cudaStream_t st);
+
+// k_sweep.cu -- Danielsson / FastSweep; `err` is a device int that receives a
+// non-zero code if a bounded wait gives up
+void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st);
+void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st);
+size_t fastsweep3_workspace_bytes(int w, int h, int d);
+void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, int* err, cudaStream_t st);
+
+}  // namespace dolk

@@ -1,0 +1,193 @@
+/*
+ * dol_b200.h -- C ABI of the B200 (sm_100a) distance-field library.
+ *
+ * A drop-in for the distance-field path of DistanceOcclusionLib
+ * (DistanceOcclusionLib.h, namespace DOL).  Every entry point takes plain
+ * pointers and sizes; the reference function each one replaces is cited
+ * beside it.  Data layouts are byte-identical to the reference's:
+ *
+ *   mask    uint32 words, each row padded to (w+31)/32 words, bit i of word j
+ *           is cell 32*j+i; rows, then slices.          (DistanceOcclusionLib.h:18-23)
+ *   deltas  dol_delta2 {int16 x,y} / dol_delta3 {int16 x,y,z}, row-major, x
+ *           fastest: the same bytes as cCellDelta2 / cCellDelta3
+ *                                                         (DistanceOcclusionLib.h:41-53)
+ *   dist    float per cell, same order.
+ *
+ * Unless a name ends in _host, every pointer argument is DEVICE memory
+ * (cudaMalloc / cudaMallocAsync / managed) and work is queued on `stream`
+ * (a cudaStream_t passed as void*; NULL is the legacy default stream).  The
+ * call returns once the work is queued; errors found before queueing are
+ * returned at once, device-side errors (a bounded wait that gave up) are
+ * reported by the next dol_sync() on that stream.  Pointers that are not
+ * device-accessible are rejected with DOL_ERR_INVALID_ARG before anything is
+ * launched.
+ *
+ * `cw` is the cell width used by the delta methods: 1 for unsigned fields
+ * initialised by dol_init_deltas_*, 2 for signed fields initialised by
+ * dol_init_border_* (deltas are then in half cells).
+ *
+ * Scratch: entry points that need temporary device memory take
+ * (void* workspace, size_t workspace_bytes).  Pass NULL/0 to let the library
+ * allocate it stream-ordered (cudaMallocAsync) and free it after the work;
+ * the dol_*_workspace_size() queries give the size to pre-allocate.
+ */
+#ifndef DOL_B200_H
+#define DOL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DOL_B200_VERSION 1
+
+#if defined(__GNUC__)
+#define DOL_API __attribute__((visibility("default")))
+#else
+#define DOL_API
+#endif
+
+typedef enum dol_status {
+    DOL_OK = 0,
+    DOL_ERR_INVALID_ARG = 1,   /* bad size, null or non-device pointer, ...      */
+    DOL_ERR_CUDA = 2,          /* a CUDA runtime call failed (see dol_last_error) */
+    DOL_ERR_NO_MEMORY = 3,     /* workspace allocation failed                     */
+    DOL_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up              */
+    DOL_ERR_UNSUPPORTED = 5,   /* size or option outside what this build handles  */
+} dol_status;
+
+typedef struct dol_delta2 { int16_t x, y; } dol_delta2;        /* == DOL::cCellDelta2 */
+typedef struct dol_delta3 { int16_t x, y, z; } dol_delta3;     /* == DOL::cCellDelta3 */
+
+#define DOL_MAX_DELTA2 32767   /* kMaxDelta2, DistanceOcclusionLib.h:56 */
+#define DOL_MAX_DELTA3 25000   /* kMaxDelta3, DistanceOcclusionLib.h:57 */
+
+/* delta propagation methods, numbered as the tool's -m (DistanceOcclusionTool.cpp:700-709) */
+typedef enum dol_method {
+    DOL_DANIELSSON = 0,
+    DOL_FASTSWEEP = 1,
+    DOL_JUMPFLOOD = 2,
+    DOL_FELZENSZWALB = 5,
+} dol_method;
+
+/* output forms of the mask-driven Felzenszwalb EDT */
+#define DOL_EDT_SQUARED 0   /* squared distance to the nearest set cell, FLT_MAX if none  */
+#define DOL_EDT_DIST    1   /* sqrtf of the above (the tool's output, Tool.cpp:753-754)   */
+#define DOL_EDT_SIGNED  2   /* dist to set cells minus dist to clear cells (the -S rule)  */
+
+/* ---- library ---------------------------------------------------------------- */
+DOL_API int         dol_version(void);
+DOL_API const char* dol_status_string(dol_status s);
+DOL_API const char* dol_last_error(void);            /* detail of the last failure on this thread */
+DOL_API dol_status  dol_sync(void* stream);          /* wait for the stream, report device errors */
+
+/* ---- bitmasks --------------------------------------------------------------- */
+/* MaskSize (DistanceOcclusionLib.h:124-135); d = 1 for images */
+DOL_API size_t dol_mask_words(int w, int h, int d);
+
+/* host-side test-mask generators, the reference's LCG and shapes
+   (BitMaskAddPoints :95-113/:1224-1244, BitMaskAddBlock :159-179/:1259-1287) */
+DOL_API void dol_add_points_2d(int w, int h, int n, uint32_t seed, uint32_t* host_mask);
+DOL_API void dol_add_points_3d(int w, int h, int d, int n, uint32_t seed, uint32_t* host_mask);
+DOL_API void dol_add_block_2d(int w, int h, int sides, uint32_t* host_mask);
+DOL_API void dol_add_block_3d(int w, int h, int d, int sides, uint32_t* host_mask);
+
+/* byte image/volume -> bitmask: bit = (v >= threshold) ^ less_than
+   (BitMaskFromImageFile, DistanceOcclusionTool.cpp:634-670) */
+DOL_API dol_status dol_pack_bytemask(int w, int h, int d, const uint8_t* bytes, int threshold, int less_than,
+                             uint32_t* mask, void* stream);
+
+/* ---- initialisation ------------------------------------------------------------ */
+/* InitDistancesFromBitMask(float) (DistanceOcclusionLib.cpp:211-222): 0 on set bits, max_d elsewhere */
+DOL_API dol_status dol_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, float max_d, void* stream);
+/* InitDeltasFromBitMask (DistanceOcclusionLib.cpp:224-254, :1289-1321) */
+DOL_API dol_status dol_init_deltas_2d(int w, int h, const uint32_t* mask, dol_delta2* deltas, int invert, void* stream);
+DOL_API dol_status dol_init_deltas_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, int invert, void* stream);
+/* InitBorderDeltasFromBitMask (DistanceOcclusionLib.cpp:604-619, :2154-2173) */
+DOL_API dol_status dol_init_border_2d(int w, int h, const uint32_t* mask, dol_delta2* deltas, void* stream);
+DOL_API dol_status dol_init_border_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, void* stream);
+
+/* ---- delta propagation (in place) ------------------------------------------------- */
+/* Danielsson (DistanceOcclusionLib.cpp:702-778, :2348-2394) */
+DOL_API dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* stream);
+DOL_API dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* stream);
+/* FastSweep (DistanceOcclusionLib.cpp:633-697, :2186-2260) */
+DOL_API dol_status dol_fastsweep_2d(int w, int h, dol_delta2* deltas, int cw, void* stream);
+DOL_API size_t     dol_fastsweep_3d_workspace_size(int w, int h, int d);
+DOL_API dol_status dol_fastsweep_3d(int w, int h, int d, dol_delta3* deltas, int cw,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* JumpFlood (DistanceOcclusionLib.cpp:887-908, :2450-2472); the workspace is
+   the reference's internal ping-pong buffer (one cell per cell) */
+DOL_API size_t     dol_jumpflood_2d_workspace_size(int w, int h);
+DOL_API size_t     dol_jumpflood_3d_workspace_size(int w, int h, int d);
+DOL_API dol_status dol_jumpflood_2d(int w, int h, dol_delta2* deltas, int cw,
+                            void* workspace, size_t workspace_bytes, void* stream);
+DOL_API dol_status dol_jumpflood_3d(int w, int h, int d, dol_delta3* deltas, int cw,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Felzenszwalb ------------------------------------------------------------------- */
+/* Felzenszwalb(w,h,float[]) (DistanceOcclusionLib.cpp:1065-1085): in-place squared
+   distance transform of an arbitrary float field, same float arithmetic */
+DOL_API size_t     dol_felzenszwalb_2d_workspace_size(int w, int h);
+DOL_API dol_status dol_felzenszwalb_2d(int w, int h, float* dist, void* workspace, size_t workspace_bytes, void* stream);
+/* Mask-driven exact EDT, the tool's InitDistancesFromBitMask + Felzenszwalb (+ sqrtf)
+   path (DistanceOcclusionTool.cpp:741-782) in 2D; the 3D form has no reference
+   counterpart (the same separable transform along z, y, x).  `form` is DOL_EDT_*. */
+DOL_API size_t     dol_edt_mask_2d_workspace_size(int w, int h);
+DOL_API size_t     dol_edt_mask_3d_workspace_size(int w, int h, int d);
+DOL_API dol_status dol_edt_mask_2d(int w, int h, const uint32_t* mask, float* out, int form,
+                           void* workspace, size_t workspace_bytes, void* stream);
+DOL_API dol_status dol_edt_mask_3d(int w, int h, int d, const uint32_t* mask, float* out, int form,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- deltas -> distances ------------------------------------------------------------ */
+/* Dist() (DistanceOcclusionTool.cpp:46-61): out = sqrtf((float)(x*x+y*y[+z*z])) / cw,
+   negated where sign_mask (nullable) has the cell's bit (Tool.cpp:1262, :1392) */
+DOL_API dol_status dol_deltas_to_dist_2d(int w, int h, const dol_delta2* deltas, int cw, const uint32_t* sign_mask,
+                                 float* out, void* stream);
+DOL_API dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* deltas, int cw,
+                                 const uint32_t* sign_mask, float* out, void* stream);
+
+/* ---- one-call fields (the tool's Generate* paths) ----------------------------------- */
+/* Signed border-initialised distance field (GenerateSignedDistanceBorder,
+   DistanceOcclusionTool.cpp:1333-1365 / :1471-1498): border init, `method`
+   with cw = 2, then signed distances.  deltas (nullable) receives the final
+   deltas; dist (nullable) the signed float distances in cells. */
+DOL_API size_t     dol_sdf_workspace_size(int w, int h, int d, int method);
+DOL_API dol_status dol_sdf_2d(int w, int h, const uint32_t* mask, int method, dol_delta2* deltas, float* dist,
+                      void* workspace, size_t workspace_bytes, void* stream);
+DOL_API dol_status dol_sdf_3d(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* deltas, float* dist,
+                      void* workspace, size_t workspace_bytes, void* stream);
+/* Same with HOST mask in and HOST outputs (either nullable); copies inside.
+   Blocks until the result is in host memory. */
+DOL_API dol_status dol_sdf_2d_host(int w, int h, const uint32_t* mask, int method, dol_delta2* deltas, float* dist);
+DOL_API dol_status dol_sdf_3d_host(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* deltas, float* dist);
+/* Mask-driven EDT with host buffers (DOL_EDT_* form) */
+DOL_API dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float* out, int form);
+
+/* ---- synthetic inputs (no reference counterpart) --------------------------------------
+   Integer-exact, so host and device give the same bits.  Value noise: lattice
+   spacing `spacing`, lattice values in [0,65536) from the reference's LCG drawn
+   x fastest; a voxel is set iff the trilinear value at (x,y,z)/spacing is >= 1/2.
+   Shapes: nbox boxes then nsph spheres, sizes in [smin,smax], integer centres;
+   a voxel is set iff its centre lies inside one.  The device forms block. */
+DOL_API dol_status dol_gen_value_noise_3d(int w, int h, int d, int spacing, uint32_t seed, uint32_t* mask, void* stream);
+DOL_API void       dol_gen_value_noise_3d_host(int w, int h, int d, int spacing, uint32_t seed, uint32_t* host_mask);
+DOL_API dol_status dol_gen_shapes_3d(int w, int h, int d, int nbox, int nsph, int smin, int smax, uint32_t seed,
+                                     uint32_t* mask, void* stream);
+DOL_API void       dol_gen_shapes_3d_host(int w, int h, int d, int nbox, int nsph, int smin, int smax, uint32_t seed,
+                                          uint32_t* host_mask);
+
+/* ---- launch profiler (no reference counterpart) -----------------------------------------
+   Between begin and end every kernel the library launches is bracketed by CUDA
+   events on its stream; end waits for them and returns up to max_entries
+   per-launch times in ms, with the kernel names '\n'-separated in `names`. */
+DOL_API void dol_profile_begin(void);
+DOL_API int  dol_profile_end(char* names, size_t names_len, float* ms, int max_entries);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOL_B200_H */

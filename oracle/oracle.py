@@ -1,0 +1,226 @@
+"""ctypes binding for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle.so`` (the C restatement in ``dol_oracle.c``) and,
+when present, ``oracle/_ref/libdolref.so`` (the unmodified reference library
+compiled by ``oracle/Makefile``).  Only tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of bench.py import this module; the CUDA library never
+does.
+
+Arrays are numpy: masks ``uint32[words]``, 2D deltas ``int16[h, w, 2]``, 3D
+deltas ``int16[d, h, w, 3]``, distances ``float32``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MAX2 = 32767
+MAX3 = 25000
+
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and _ref/libdolref.so when the reference sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = C.CDLL(path)
+    return _lib
+
+
+def ref():
+    """The reference library build, or None when oracle/_ref was not built."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libdolref.so")
+        if not os.path.exists(path):
+            return None
+        _ref = C.CDLL(path)
+    return _ref
+
+
+def mask_words(w, h, d=1):
+    return ((w + 31) // 32) * h * d
+
+
+def new_mask(w, h, d=1):
+    return np.zeros(mask_words(w, h, d), dtype=np.uint32)
+
+
+def _i(*xs):
+    return [C.c_int(int(x)) for x in xs]
+
+
+# ---- generators ---------------------------------------------------------------
+
+def add_points(mask, dims, n, seed, use_ref=False):
+    L = ref() if use_ref else lib()
+    pre = "ref_" if use_ref else "dolo_"
+    if len(dims) == 2:
+        getattr(L, pre + "add_points_2d")(*_i(*dims, n), C.c_uint32(seed), _p(mask))
+    else:
+        getattr(L, pre + "add_points_3d")(*_i(*dims, n), C.c_uint32(seed), _p(mask))
+    return mask
+
+
+def add_block(mask, dims, sides, use_ref=False):
+    L = ref() if use_ref else lib()
+    pre = "ref_" if use_ref else "dolo_"
+    fn = getattr(L, pre + ("add_block_2d" if len(dims) == 2 else "add_block_3d"))
+    fn(*_i(*dims, sides), _p(mask))
+    return mask
+
+
+def pack_bytes(img, threshold=128, less_than=True):
+    h, w = img.shape
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    m = new_mask(w, h)
+    lib().dolo_pack_bytes(*_i(w, h), _p(img), *_i(threshold, 1 if less_than else 0), _p(m))
+    return m
+
+
+# ---- delta methods --------------------------------------------------------------
+
+def _deltas(dims):
+    if len(dims) == 2:
+        w, h = dims
+        return np.empty((h, w, 2), dtype=np.int16)
+    w, h, d = dims
+    return np.empty((d, h, w, 3), dtype=np.int16)
+
+
+def init_deltas(mask, dims, invert=False, use_ref=False):
+    out = _deltas(dims)
+    nd = len(dims)
+    if use_ref:
+        getattr(ref(), f"ref_init_deltas_{nd}d")(*_i(*dims), _p(mask), _p(out), C.c_int(int(invert)))
+    else:
+        getattr(lib(), f"dolo_init_deltas_{nd}d")(*_i(*dims), _p(mask), _p(out), C.c_int(int(invert)))
+    return out
+
+
+def border_init(mask, dims, use_ref=False):
+    out = _deltas(dims)
+    nd = len(dims)
+    name = ("ref_" if use_ref else "dolo_") + f"border_init_{nd}d"
+    getattr(ref() if use_ref else lib(), name)(*_i(*dims), _p(mask), _p(out))
+    return out
+
+
+def propagate(method, deltas, dims, cw, use_ref=False, exact_bf3=False):
+    """Run a delta method in place on a copy; returns the new array."""
+    out = np.ascontiguousarray(deltas).copy()
+    nd = len(dims)
+    if use_ref:
+        fn = getattr(ref(), f"ref_{method}_{nd}d")
+        fn(*_i(*dims), _p(out), C.c_int(cw))
+        return out
+    L = lib()
+    if method == "jumpflood":
+        tmp = np.empty_like(out)
+        getattr(L, f"dolo_jumpflood_{nd}d")(*_i(*dims), _p(out), C.c_int(cw), _p(tmp))
+    elif method == "bruteforce" and nd == 3:
+        L.dolo_bruteforce_3d(*_i(*dims), _p(out), C.c_int(cw), C.c_int(1 if exact_bf3 else 0))
+    else:
+        getattr(L, f"dolo_{method}_{nd}d")(*_i(*dims), _p(out), C.c_int(cw))
+    return out
+
+
+def deltas_to_dist(deltas, dims, cw, sign_mask=None):
+    nd = len(dims)
+    out = np.empty(deltas.shape[:-1], dtype=np.float32)
+    sm = _p(sign_mask) if sign_mask is not None else None
+    getattr(lib(), f"dolo_deltas_to_dist_{nd}d")(*_i(*dims), _p(np.ascontiguousarray(deltas)),
+                                                 C.c_int(cw), sm, _p(out))
+    return out
+
+
+# ---- Felzenszwalb ---------------------------------------------------------------------
+
+def init_distances(mask, dims, use_ref=False):
+    w, h = dims
+    out = np.empty((h, w), dtype=np.float32)
+    if use_ref:
+        ref().ref_init_distances_2d(*_i(w, h), _p(mask), _p(out))
+    else:
+        lib().dolo_init_distances_2d(*_i(w, h), _p(mask), _p(out), C.c_float(np.finfo(np.float32).max))
+    return out
+
+
+def felzenszwalb(dist, dims, use_ref=False, threads=1):
+    """Squared EDT of a float field (0 at seeds, FLT_MAX elsewhere), in place on a copy."""
+    out = np.ascontiguousarray(dist, dtype=np.float32).copy()
+    n = max(dims)
+    if use_ref:
+        if len(dims) == 2:
+            ref().ref_felzenszwalb_2d(*_i(*dims), _p(out))
+        else:
+            ref().ref_felzenszwalb_3d(*_i(*dims), _p(out), C.c_int(threads))
+        return out
+    v = np.empty(n, dtype=np.int32)
+    z = np.empty(n + 1, dtype=np.float32)
+    if len(dims) == 2:
+        td = np.empty(out.size, dtype=np.float32)
+        lib().dolo_felzenszwalb_2d(*_i(*dims), _p(out), _p(td), _p(v), _p(z))
+    else:
+        td = np.empty(n, dtype=np.float32)
+        lib().dolo_felzenszwalb_3d(*_i(*dims), _p(out), _p(td), _p(v), _p(z))
+    return out
+
+
+def mask_to_bool(mask, dims):
+    """Unpack a padded bitmask to bool[h, w] / bool[d, h, w]."""
+    w = dims[0]
+    ws = (w + 31) // 32
+    rows = mask.reshape(-1, ws)
+    bits = np.unpackbits(rows.view(np.uint8).reshape(rows.shape[0], ws * 4), axis=1, bitorder="little")
+    b = bits[:, :w].astype(bool)
+    return b.reshape(tuple(reversed(dims)))
+
+
+def bool_to_mask(b):
+    """Pack bool[h, w] / bool[d, h, w] (x fastest) into a padded bitmask."""
+    b = np.asarray(b, dtype=bool)
+    w = b.shape[-1]
+    ws = (w + 31) // 32
+    rows = b.reshape(-1, w)
+    pad = np.zeros((rows.shape[0], ws * 32), dtype=np.uint8)
+    pad[:, :w] = rows
+    packed = np.packbits(pad, axis=1, bitorder="little")
+    return np.ascontiguousarray(packed).view(np.uint32).reshape(-1).copy()
+
+
+def sdf_signed_felzenszwalb(mask, dims):
+    """Two-pass signed Felzenszwalb (distance to occupied minus distance to empty),
+    the orthodox -S convention of DistanceOcclusionTool.cpp:1036, built from the
+    restated EDT: positive outside, negative inside."""
+    b = mask_to_bool(mask, dims)
+    big = np.float32(np.finfo(np.float32).max)
+    f_occ = np.where(b, np.float32(0), big).astype(np.float32)
+    f_emp = np.where(b, big, np.float32(0)).astype(np.float32)
+    e_occ = felzenszwalb(f_occ, dims)
+    e_emp = felzenszwalb(f_emp, dims)
+    return (np.sqrt(e_occ) - np.sqrt(e_emp)).astype(np.float32)
+
+
+def edt_brute(mask, dims):
+    d3 = list(dims) + [1] * (3 - len(dims))
+    out = np.empty(d3[0] * d3[1] * d3[2], dtype=np.float32)
+    lib().dolo_edt_brute(*_i(*d3), _p(mask), _p(out))
+    return out.reshape(tuple(reversed(dims)))

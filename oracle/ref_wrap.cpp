@@ -1,0 +1,85 @@
+/*
+ * ref_wrap.cpp -- C entry points into the UNMODIFIED reference library.
+ *
+ * TEST / BASELINE INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file
+ * with -I pointing at the reference checkout, so the translation unit below
+ * includes DistanceOcclusionLib.cpp exactly as it lies there (built with the
+ * reference's own -O3, no OpenMP, as its Makefile does).  Including the .cpp
+ * rather than linking it gives access to the file-local 1D Felzenszwalb
+ * routine (DistanceOcclusionLib.cpp:1026-1062), which the 3D restatement below
+ * applies along z, y and x -- the reference has no 3D Felzenszwalb.
+ *
+ * The output, oracle/_ref/libdolref.so, is git-ignored and never shipped; it
+ * pins the C restatement in dol_oracle.c and serves as the timed CPU
+ * baseline ("kind": "reference").
+ */
+#include "DistanceOcclusionLib.cpp"
+
+#include <thread>
+#include <vector>
+
+extern "C" {
+
+void ref_add_points_2d(int w, int h, int n, uint32_t seed, uint32_t* mask) { DOL::BitMaskAddPoints(w, h, n, seed, mask); }
+void ref_add_points_3d(int w, int h, int d, int n, uint32_t seed, uint32_t* mask) { DOL::BitMaskAddPoints(w, h, d, n, seed, mask); }
+void ref_add_block_2d(int w, int h, int sides, uint32_t* mask) { DOL::BitMaskAddBlock(w, h, sides, mask); }
+void ref_add_block_3d(int w, int h, int d, int sides, uint32_t* mask) { DOL::BitMaskAddBlock(w, h, d, sides, mask); }
+
+void ref_init_distances_2d(int w, int h, const uint32_t* mask, float* dist) { DOL::InitDistancesFromBitMask(w, h, mask, dist); }
+void ref_init_deltas_2d(int w, int h, const uint32_t* mask, DOL::cCellDelta2* dl, int invert) { DOL::InitDeltasFromBitMask(w, h, mask, dl, invert != 0); }
+void ref_init_deltas_3d(int w, int h, int d, const uint32_t* mask, DOL::cCellDelta3* dl, int invert) { DOL::InitDeltasFromBitMask(w, h, d, mask, dl, invert != 0); }
+void ref_border_init_2d(int w, int h, const uint32_t* mask, DOL::cCellDelta2* dl) { DOL::InitBorderDeltasFromBitMask(w, h, mask, dl); }
+void ref_border_init_3d(int w, int h, int d, const uint32_t* mask, DOL::cCellDelta3* dl) { DOL::InitBorderDeltasFromBitMask(w, h, d, mask, dl); }
+
+void ref_danielsson_2d(int w, int h, DOL::cCellDelta2* dl, int cw) { DOL::Danielsson(w, h, dl, cw); }
+void ref_danielsson_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::Danielsson(w, h, d, dl, cw); }
+void ref_fastsweep_2d(int w, int h, DOL::cCellDelta2* dl, int cw) { DOL::FastSweep(w, h, dl, cw); }
+void ref_fastsweep_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::FastSweep(w, h, d, dl, cw); }
+void ref_jumpflood_2d(int w, int h, DOL::cCellDelta2* dl, int cw) { DOL::JumpFlood(w, h, dl, cw); }
+void ref_jumpflood_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::JumpFlood(w, h, d, dl, cw); }
+void ref_bruteforce_2d(int w, int h, DOL::cCellDelta2* dl, int cw) { DOL::BruteForce(w, h, dl, cw); }
+void ref_bruteforce_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::BruteForce(w, h, d, dl, cw); }
+void ref_felzenszwalb_2d(int w, int h, float* dist) { DOL::Felzenszwalb(w, h, dist); }
+
+/* 3D restatement on the reference's own 1D routine: z, then y, then x.  Lines
+ * are split over `threads` host threads, each with private v/z/line scratch
+ * (the reference's OpenMP pragmas share that scratch, so they are not used). */
+void ref_felzenszwalb_3d(int w, int h, int d, float* dist, int threads)
+{
+    if (threads < 1) threads = 1;
+    const size_t ss = (size_t)w * h;
+    const int nmax = (w > h ? (w > d ? w : d) : (h > d ? h : d));
+
+    auto run = [&](int pass, int t) {
+        std::vector<int> v(nmax);
+        std::vector<float> z(nmax + 1), line(nmax);
+        if (pass == 0) {            /* along z: lines indexed by (y, x) */
+            for (size_t c = t; c < ss; c += threads) {
+                float* col = dist + c;
+                ::Felzenszwalb(d, (int)ss, col, line.data(), v.data(), z.data());
+                for (int q = 0; q < d; q++) col[(size_t)q * ss] = line[q];
+            }
+        } else if (pass == 1) {     /* along y: lines indexed by (z, x) */
+            for (size_t c = t; c < (size_t)d * w; c += threads) {
+                size_t k = c / w, x = c % w;
+                float* col = dist + k * ss + x;
+                ::Felzenszwalb(h, w, col, line.data(), v.data(), z.data());
+                for (int q = 0; q < h; q++) col[(size_t)q * w] = line[q];
+            }
+        } else {                    /* along x: lines indexed by (z, y) */
+            for (size_t c = t; c < (size_t)d * h; c += threads) {
+                float* row = dist + c * w;
+                ::Felzenszwalb(w, 1, row, line.data(), v.data(), z.data());
+                for (int q = 0; q < w; q++) row[q] = line[q];
+            }
+        }
+    };
+    for (int pass = 0; pass < 3; pass++) {
+        if (threads == 1) { run(pass, 0); continue; }
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; t++) pool.emplace_back(run, pass, t);
+        for (auto& th : pool) th.join();
+    }
+}
+
+}  /* extern "C" */

@@ -1,0 +1,213 @@
+"""GPU parity: every entry point of the CUDA library against the CPU oracle on
+the same inputs, through the C ABI.  Integer outputs (masks, deltas) must be
+bit-exact; float outputs are compared bit-for-bit as well, because every float
+the reference produces on this path is a correctly rounded function of an
+integer (sqrtf of an exact squared length, or the exact squared EDT)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def dev(torch, a):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint32:
+        a = a.view(np.int32)
+    return torch.from_numpy(a).cuda()
+
+
+def host(t):
+    a = t.cpu().numpy()
+    return a.view(np.uint32) if a.dtype == np.int32 else a
+
+
+def same_float(a, b):
+    """bitwise equal, treating any NaN as equal to any NaN"""
+    a, b = np.asarray(a, np.float32), np.asarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb)
+    assert np.array_equal(a.view(np.uint32)[~na], b.view(np.uint32)[~nb])
+
+
+def rand_mask(O, rng, dims, p):
+    return O.bool_to_mask(rng.random(tuple(reversed(dims))) < p)
+
+
+SHAPES2 = [(1, 1), (1, 9), (9, 1), (31, 7), (32, 8), (33, 13), (64, 64), (100, 37), (257, 19), (1000, 5)]
+SHAPES3 = [(1, 1, 1), (5, 1, 1), (1, 4, 3), (9, 7, 5), (32, 3, 4), (33, 6, 5), (40, 1, 6), (24, 20, 16)]
+PS = (0.0, 0.01, 0.2, 0.6, 1.0)
+
+
+@pytest.mark.parametrize("dims", SHAPES2 + SHAPES3)
+def test_init_and_border(dol, O, cuda, dims):
+    rng = np.random.default_rng(sum(dims))
+    for p in PS:
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        for inv in (False, True):
+            np.testing.assert_array_equal(host(dol.init_deltas(md, dims, inv)), O.init_deltas(m, dims, inv))
+        np.testing.assert_array_equal(host(dol.init_border(md, dims)), O.border_init(m, dims), err_msg=f"p={p}")
+        if len(dims) == 2:
+            same_float(host(dol.init_distances(md, dims)), O.init_distances(m, dims))
+
+
+@pytest.mark.parametrize("method", ["danielsson", "fastsweep", "jumpflood"])
+@pytest.mark.parametrize("dims", SHAPES2 + SHAPES3)
+def test_delta_methods(dol, O, cuda, dims, method):
+    rng = np.random.default_rng(sum(dims) + len(method))
+    for p in PS:
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        for cw in (1, 2):
+            start = O.init_deltas(m, dims) if cw == 1 else O.border_init(m, dims)
+            want = O.propagate(method, start, dims, cw)
+            got = dol.propagate(method, dev(cuda, start), dims, cw)
+            dol.sync()
+            np.testing.assert_array_equal(host(got), want, err_msg=f"{method} cw{cw} p{p} dims{dims}")
+
+
+@pytest.mark.parametrize("dims", [(1024, 1024)])
+def test_config1_against_reference_digests(dol, O, cuda, dims):
+    with open(os.path.join(HERE, "golden", "golden_digests.json")) as f:
+        dig = json.load(f)
+    m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+    assert hashlib.sha256(m.tobytes()).hexdigest() == dig["c1_mask"]
+    md = dev(cuda, m)
+    for method in ("danielsson", "fastsweep", "jumpflood"):
+        got = host(dol.propagate(method, dol.init_deltas(md, dims), dims, 1))
+        assert hashlib.sha256(got.tobytes()).hexdigest() == dig[f"c1_{method}_cw1"], method
+        got = host(dol.propagate(method, dol.init_border(md, dims), dims, 2))
+        assert hashlib.sha256(got.tobytes()).hexdigest() == dig[f"c1_{method}_cw2"], method
+    sq = host(dol.edt_mask(md, dims, dol.EDT_SQUARED))
+    assert hashlib.sha256(sq.tobytes()).hexdigest() == dig["c1_felz"]
+
+
+def test_volume64_against_reference_digests(dol, O, cuda):
+    with open(os.path.join(HERE, "golden", "golden_digests.json")) as f:
+        dig = json.load(f)
+    dims = (64, 64, 64)
+    m = dol.add_points(dol.add_block(np.zeros(dol.mask_words(*dims), np.uint32), dims, 6), dims, 200, 12345)
+    assert hashlib.sha256(m.tobytes()).hexdigest() == dig["v64_mask"]
+    md = dev(cuda, m)
+    bor = dol.init_border(md, dims)
+    assert hashlib.sha256(host(bor).tobytes()).hexdigest() == dig["v64_border"]
+    for method in ("danielsson", "fastsweep", "jumpflood"):
+        got = host(dol.propagate(method, dol.init_border(md, dims), dims, 2))
+        dol.sync()
+        assert hashlib.sha256(got.tobytes()).hexdigest() == dig[f"v64_{method}_cw2"], method
+        got = host(dol.propagate(method, dol.init_deltas(md, dims), dims, 1))
+        assert hashlib.sha256(got.tobytes()).hexdigest() == dig[f"v64_{method}_cw1"], method
+
+
+@pytest.mark.parametrize("dims", SHAPES2 + SHAPES3 + [(300, 200), (70, 60, 50)])
+def test_edt_mask_forms(dol, O, cuda, dims):
+    rng = np.random.default_rng(sum(dims) + 99)
+    big = np.float32(np.finfo(np.float32).max)
+    for p in (0.0, 0.003, 0.05, 0.5, 1.0):
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        b = O.mask_to_bool(m, dims)
+        want_sq = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SQUARED)), want_sq)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_DIST)), np.sqrt(want_sq))
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
+
+
+@pytest.mark.parametrize("dims", [(1, 1), (7, 1), (1, 7), (33, 17), (64, 48), (200, 130)])
+def test_felzenszwalb_float_field(dol, O, cuda, dims):
+    """DOL::Felzenszwalb on arbitrary floats, not just 0 / FLT_MAX."""
+    rng = np.random.default_rng(sum(dims))
+    w, h = dims
+    big = np.float32(np.finfo(np.float32).max)
+    for kind in range(3):
+        if kind == 0:
+            f = (rng.random((h, w)) * 50).astype(np.float32)
+        elif kind == 1:
+            f = np.where(rng.random((h, w)) < 0.1, (rng.random((h, w)) * 3).astype(np.float32), big)
+        else:
+            f = np.where(rng.random((h, w)) < 0.02, np.float32(0), big).astype(np.float32)
+        want = O.felzenszwalb(f, dims)
+        got = dol.felzenszwalb(dev(cuda, f.astype(np.float32)), dims)
+        same_float(host(got), want)
+
+
+@pytest.mark.parametrize("dims", SHAPES2 + SHAPES3)
+def test_deltas_to_dist(dol, O, cuda, dims):
+    rng = np.random.default_rng(sum(dims) + 3)
+    m = rand_mask(O, rng, dims, 0.2)
+    for cw, start in ((1, O.init_deltas(m, dims)), (2, O.border_init(m, dims))):
+        dl = O.propagate("danielsson", start, dims, cw)
+        for sign in (None, m):
+            want = O.deltas_to_dist(dl, dims, cw, sign)
+            got = dol.deltas_to_dist(dev(cuda, dl), dims, cw, None if sign is None else dev(cuda, sign))
+            same_float(host(got), want)
+
+
+@pytest.mark.parametrize("dims", [(1, 1), (33, 5), (100, 37), (64, 8, 5)])
+def test_pack_bytemask(dol, O, cuda, dims):
+    rng = np.random.default_rng(sum(dims))
+    img = rng.integers(0, 256, size=tuple(reversed(dims)), dtype=np.uint8)
+    for thr, lt in ((128, True), (128, False), (0, True), (255, False)):
+        got = host(dol.pack_bytemask(dev(cuda, img), thr, lt))
+        if len(dims) == 2:
+            want = O.pack_bytes(img, thr, lt)
+        else:
+            want = O.pack_bytes(img.reshape(-1, dims[0]), thr, lt)
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("method", ["danielsson", "fastsweep", "jumpflood", "felzenszwalb"])
+@pytest.mark.parametrize("dims", [(64, 48), (33, 20, 17)])
+def test_sdf_pipeline_device_and_host(dol, O, cuda, dims, method):
+    rng = np.random.default_rng(7)
+    m = rand_mask(O, rng, dims, 0.3)
+    if method == "felzenszwalb":
+        want_dl, want_df = None, O.sdf_signed_felzenszwalb(m, dims)
+    else:
+        want_dl = O.propagate(method, O.border_init(m, dims), dims, 2)
+        want_df = O.deltas_to_dist(want_dl, dims, 2, m)
+    dl, df = dol.sdf(dev(cuda, m), dims, method)
+    dol.sync()
+    if want_dl is not None:
+        np.testing.assert_array_equal(host(dl), want_dl)
+    same_float(host(df), want_df)
+    hdl, hdf = dol.sdf_host(m, dims, method)
+    if want_dl is not None:
+        np.testing.assert_array_equal(hdl, want_dl)
+    same_float(hdf, want_df)
+
+
+def test_word_boundary_single_seeds(dol, O, cuda):
+    """A lone set cell at x = 30, 31, 32 exercises the cross-word write order
+    of the border initialisation (the x = 31 case ends as (1, 0))."""
+    for dims in [(64, 4), (96, 3), (64, 3, 3)]:
+        for x in (0, 30, 31, 32, 33, 63):
+            b = np.zeros(tuple(reversed(dims)), bool)
+            if len(dims) == 2:
+                b[1, x] = True
+            else:
+                b[1, 1, x] = True
+            m = O.bool_to_mask(b)
+            got = host(dol.init_border(dev(cuda, m), dims))
+            np.testing.assert_array_equal(got, O.border_init(m, dims), err_msg=f"x={x} {dims}")
+
+
+def test_rejects_bad_arguments(dol, cuda):
+    import ctypes as C
+    L = dol.lib()
+    buf = cuda.zeros(64, dtype=cuda.int32, device="cuda")
+    hostbuf = np.zeros(64, np.uint32)
+    st = L.dol_init_border_2d(C.c_int(32), C.c_int(2), hostbuf.ctypes.data_as(C.c_void_p),
+                              C.c_void_p(buf.data_ptr()), None)
+    assert st == dol.ERR_INVALID_ARG
+    st = L.dol_init_border_2d(C.c_int(0), C.c_int(2), C.c_void_p(buf.data_ptr()), C.c_void_p(buf.data_ptr()), None)
+    assert st == dol.ERR_INVALID_ARG
+    st = L.dol_danielsson_2d(C.c_int(5000), C.c_int(2), C.c_void_p(buf.data_ptr()), C.c_int(1), None)
+    assert st == dol.ERR_UNSUPPORTED
+    with pytest.raises(dol.DolError):
+        dol.edt_mask(buf, (32, 2), form=7)

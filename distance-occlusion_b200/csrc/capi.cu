@@ -140,8 +140,10 @@ dol_status get_workspace(Workspace& ws, void* user, size_t user_bytes, size_t ne
 
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
-// widest row the single-CTA sweeps handle (8 cells per thread, 512 threads)
+// widest row the single-CTA sweeps handle (8 cells per thread, 512 threads),
+// and the 3D FastSweep wavefront (8 cells per thread, 256 threads)
 constexpr int kMaxSweepWidth = 4096;
+constexpr int kMaxSweepWidth3 = 2048;
 
 dol_status check_sweep_width(int w)
 {
@@ -376,6 +378,7 @@ dol_status dol_fastsweep_3d(int w, int h, int d, dol_delta3* deltas, int cw, voi
     DOL_TRY(check_dims(w, h, d));
     DOL_TRY(check_cw(cw));
     DOL_TRY(check_sweep_width(w));
+    if (w > kMaxSweepWidth3) return fail(DOL_ERR_UNSUPPORTED, "3D FastSweep rows are limited to %d cells", kMaxSweepWidth3);
     DOL_TRY(check_dev_ptr(deltas, "deltas"));
     Workspace ws;
     DOL_TRY(get_workspace(ws, workspace, workspace_bytes, fastsweep3_workspace_bytes(w, h, d), S(stream)));
@@ -407,6 +410,7 @@ dol_status dol_jumpflood_3d(int w, int h, int d, dol_delta3* deltas, int cw, voi
     DOL_TRY(device_state(&ds));
     DOL_TRY(check_dims(w, h, d));
     DOL_TRY(check_cw(cw));
+    if (d > 65535) return fail(DOL_ERR_UNSUPPORTED, "JumpFlood volumes are limited to 65535 slices");
     DOL_TRY(check_dev_ptr(deltas, "deltas"));
     Workspace ws;
     DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_jumpflood_3d_workspace_size(w, h, d), S(stream)));
@@ -524,6 +528,10 @@ static dol_status sdf_common(int dim, int w, int h, int d, const uint32_t* mask,
     if (method == DOL_FELZENSZWALB && deltas)
         return fail(DOL_ERR_INVALID_ARG, "Felzenszwalb produces distances only; pass deltas = NULL");
     if (method == DOL_DANIELSSON || method == DOL_FASTSWEEP) DOL_TRY(check_sweep_width(w));
+    if (method == DOL_FASTSWEEP && dim == 3 && w > kMaxSweepWidth3)
+        return fail(DOL_ERR_UNSUPPORTED, "3D FastSweep rows are limited to %d cells", kMaxSweepWidth3);
+    if (method == DOL_JUMPFLOOD && dim == 3 && d > 65535)
+        return fail(DOL_ERR_UNSUPPORTED, "JumpFlood volumes are limited to 65535 slices");
     cudaStream_t st = S(stream);
     Workspace ws;
     DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_sdf_workspace_size(w, h, dim == 3 ? d : 1, method), st));

@@ -274,12 +274,16 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
 
 // --------------------------------------------------------------- launchers ----
 
+// cells per thread: aim for at most 256 threads (fewer warps at every barrier),
+// allow up to max_threads for wide rows; 0 when the row is too wide
 static int pick_s(int w, int max_threads)
 {
     const int options[] = {1, 2, 4, 8};
     for (int s : options)
-        if ((w + s - 1) / s <= max_threads && ((w + s - 1) / s > 64 || s == 1 || w <= 64 * s)) return s;
-    return (w + 7) / 8 <= max_threads ? 8 : 0;
+        if ((w + s - 1) / s <= 256 && (w + s - 1) / s <= max_threads) return s;
+    for (int s : options)
+        if ((w + s - 1) / s <= max_threads) return s;
+    return 0;
 }
 
 static int threads_for(int w, int s)

@@ -150,7 +150,9 @@ __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t
             const int gap = (dir > 0 ? t - j : j - t) - 1;   // full segments in between
             nin = addx(sh.out[b][j], -dir * cw * S * gap);
         }
-        if (!__syncthreads_or(bad)) break;
+        // the fixed point is reached within nseg rounds; the cap only guards
+        // against a logic error turning into an endless loop on the device
+        if (!__syncthreads_or(bad) || r > nseg + 2) break;
         in = nin;
     }
 }

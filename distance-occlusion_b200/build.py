@@ -2,7 +2,7 @@
 
 Usage:  python distance-occlusion_b200/build.py [--force] [--verbose]
 
-Every .cu file under csrc/ is compiled for sm_100a (-gencode
+Every .cu file under csrc/ (and the C++ host interface in shim/) is compiled for sm_100a (-gencode
 arch=compute_100a,code=sm_100a) with -lineinfo and linked with the static CUDA
 runtime into distance-occlusion_b200/libdol_b200.so.  The object files go to
 distance-occlusion_b200/_build/ and are rebuilt only when a source or header
@@ -37,14 +37,14 @@ def _newest(paths):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    sources = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + sorted(glob.glob(os.path.join(PKG, "shim", "*.cpp")))
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+        glob.glob(os.path.join(ROOT, "include", "*.h")) + glob.glob(os.path.join(PKG, "shim", "*.h"))
     hdr_time = _newest(headers)
     objs = []
     jobs = []
     for src in sources:
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(BUILD, os.path.splitext(os.path.basename(src))[0] + ".o")
         objs.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_time):
             cmd = [NVCC] + FLAGS + ["-Xptxas", "-v"] * bool(verbose) + ["-c", src, "-o", obj]

@@ -60,11 +60,12 @@ DOL_HD void cell_store(int16_t* p, long long i, C3 c)
 
 // Segment-local serial pass.  dir = +1: cells 0..n-1, chain shift -cw;
 // dir = -1: cells n-1..0, chain shift +cw (a template argument, so the
-// register arrays stay in registers).  `diag` (FastSweep 2D) supplies the
-// previous-row candidate for every cell except the first of the whole row.
+// register arrays stay in registers).  D (FastSweep 2D) holds the
+// previous-row diagonal candidate of each cell; like the chain candidate it
+// exists for every cell but the first of the row in scan order.
 template <class Cell, int S, bool kDiag, int dir>
 __device__ __forceinline__ Cell seg_pass(Cell (&R)[S], const Cell (&V)[S], int n, int cw, Cell in, bool has_in,
-                                         const Cell (&D)[S], bool first_has_diag)
+                                         const Cell (&D)[S])
 {
     Cell cur = in;
     bool have = has_in;
@@ -73,8 +74,12 @@ __device__ __forceinline__ Cell seg_pass(Cell (&R)[S], const Cell (&V)[S], int n
         const int s = dir > 0 ? u : S - 1 - u;
         if (s < n) {
             Cell v = V[s];
-            if (have) v = closer(v, addx(cur, -dir * cw));
-            if (kDiag && (u > 0 || first_has_diag)) v = closer(v, D[s]);
+            // both the chain and the diagonal candidate exist iff a cell precedes
+            // this one in the row's scan order
+            if (have) {
+                v = closer(v, addx(cur, -dir * cw));
+                if (kDiag) v = closer(v, D[s]);
+            }
             R[s] = v;
             cur = v;
             have = true;
@@ -95,8 +100,7 @@ __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t
     const int sigma = dir > 0 ? t : nseg - 1 - t;
     const int pred = t - dir;
     const bool has_pred = active && sigma > 0;
-    // FastSweep: the first cell of the row in scan order has no diagonal candidate
-    const bool first_diag = has_pred || row_first_diag_ok;
+    (void)row_first_diag_ok;
 
     // round 0 guess: the predecessor's boundary cell before the pass
     Cell edge = V[0];
@@ -112,7 +116,7 @@ __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t
 
     for (int r = 0;; r++) {
         const int b = r & 1;
-        Cell out = seg_pass<Cell, S, kDiag, dir>(R, V, n, cw, in, has_in, D, first_diag);
+        Cell out = seg_pass<Cell, S, kDiag, dir>(R, V, n, cw, in, has_in, D);
         const bool trans = has_in && same(out, addx(in, -dir * cw * n));
         if (active) sh.out[b][t] = out;
         const uint32_t nt = __ballot_sync(0xFFFFFFFFu, active && !trans);

@@ -451,7 +451,7 @@ static dol_status edt_common(int dim, int w, int h, int d, const uint32_t* mask,
     DOL_TRY(check_dev_ptr(out, "out"));
     Workspace ws;
     DOL_TRY(get_workspace(ws, workspace, workspace_bytes, edt_workspace_bytes(dim, w, h, d), S(stream)));
-    launch_edt_mask(dim, mask, out, w, h, d, form, ws.ptr, S(stream));
+    launch_edt_mask(dim, mask, out, w, h, d, form, ws.ptr, ds->err_dev, S(stream));
     return launched("edt_mask");
 }
 
@@ -537,7 +537,7 @@ static dol_status sdf_common(int dim, int w, int h, int d, const uint32_t* mask,
     DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_sdf_workspace_size(w, h, dim == 3 ? d : 1, method), st));
 
     if (method == DOL_FELZENSZWALB) {
-        launch_edt_mask(dim, mask, dist, w, h, d, DOL_EDT_SIGNED, ws.ptr, st);
+        launch_edt_mask(dim, mask, dist, w, h, d, DOL_EDT_SIGNED, ws.ptr, ds->err_dev, st);
         return launched("sdf (felzenszwalb)");
     }
     const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);

@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 #ifndef DOL_EDT_SQUARED
 #define DOL_EDT_SQUARED 0
@@ -171,6 +172,45 @@ __device__ __forceinline__ float final_value(uint32_t state, uint32_t best, int 
     return form == DOL_EDT_DIST ? sqrtf(e) : e;
 }
 
+// min over the line of (q-q')^2 + f(q') for the cell at q, walking outwards
+// until k^2 reaches the best value found (f >= 0 makes that exact)
+template <typename TIn, class At>
+__device__ __forceinline__ uint32_t search_line(const At& at, int q, int n, uint32_t* state)
+{
+    uint32_t s, best;
+    decode_in<TIn>(at(q), &s, &best);
+    const int reach = max(q, n - 1 - q);
+    for (int k = 1; k <= reach; k++) {
+        const uint32_t k2 = (uint32_t)k * (uint32_t)k;
+        if (k2 >= best) break;
+        if (q - k >= 0) {
+            uint32_t s2, f;
+            decode_in<TIn>(at(q - k), &s2, &f);
+            best = min(best, s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2));
+        }
+        if (q + k < n) {
+            uint32_t s2, f;
+            decode_in<TIn>(at(q + k), &s2, &f);
+            best = min(best, s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2));
+        }
+    }
+    *state = s;
+    return best;
+}
+
+template <bool kFinal>
+__device__ __forceinline__ void put_line_value(void* out, long long o, uint32_t s, uint32_t best, int form)
+{
+    if (kFinal) {
+        static_cast<float*>(out)[o] = final_value(s, best, form);
+    } else {
+        uint32_t e = best == 0xFFFFFFFFu ? kInf32 : best;
+        static_cast<uint32_t*>(out)[o] = e | (s << 31);
+    }
+}
+
+// Plain-load form: 32 adjacent x per CTA, the line staged in shared memory when
+// it fits (kStaged) or read from global memory otherwise.
 template <typename TIn, bool kFinal, bool kStaged>
 __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, void* __restrict__ out, int w, int n,
                                                   long long stride, long long outer_stride, int form)
@@ -187,53 +227,127 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
         __syncthreads();
     }
     auto at = [&](int q) -> TIn { return kStaged ? tile[q * 32 + lane] : in[base + q * stride]; };
-
     for (int q = wib; q < n; q += nw) {
         if (!live) continue;
-        uint32_t s, best;
-        decode_in<TIn>(at(q), &s, &best);
-        const int reach = max(q, n - 1 - q);
-        for (int k = 1; k <= reach; k++) {
-            uint32_t k2 = (uint32_t)k * (uint32_t)k;
-            if (k2 >= best) break;
-            if (q - k >= 0) {
-                uint32_t s2, f;
-                decode_in<TIn>(at(q - k), &s2, &f);
-                uint32_t c = s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2);
-                best = min(best, c);
-            }
-            if (q + k < n) {
-                uint32_t s2, f;
-                decode_in<TIn>(at(q + k), &s2, &f);
-                uint32_t c = s2 != s ? k2 : (f == 0xFFFFFFFFu ? f : f + k2);
-                best = min(best, c);
-            }
+        uint32_t s;
+        uint32_t best = search_line<TIn>(at, q, n, &s);
+        put_line_value<kFinal>(out, base + q * stride, s, best, form);
+    }
+}
+
+// TMA form: a 16-column x full-line tile arrives in 256-position boxes
+// (cp.async.bulk.tensor, one mbarrier); lanes 0-15 and 16-31 of a warp take
+// two adjacent positions of the 16 columns.  Several CTAs per SM overlap one
+// tile's load with another's search.
+template <typename TIn, bool kFinal>
+__global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
+                                                      int w, int n, long long stride, long long outer_stride,
+                                                      int along_z, int form, int* err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TIn* tile = reinterpret_cast<TIn*>(smem_raw);   // [boxes * 256][16]
+    __shared__ __align__(8) uint64_t bar;
+    const int x0 = blockIdx.x * 16;
+    const int outer = blockIdx.y;
+    const int nbox = (n + 255) >> 8;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (uint32_t)(nbox * 256 * 16 * sizeof(TIn)));
+        for (int b = 0; b < nbox; b++) {
+            if (along_z)
+                tma_load_3d(tile + b * 256 * 16, &map, x0, outer, b * 256, &bar);
+            else
+                tma_load_3d(tile + b * 256 * 16, &map, x0, b * 256, outer, &bar);
         }
-        long long o = base + q * stride;
-        if (kFinal) {
-            static_cast<float*>(out)[o] = final_value(s, best, form);
-        } else {
-            uint32_t e = best == 0xFFFFFFFFu ? kInf32 : best;
-            static_cast<uint32_t*>(out)[o] = e | (s << 31);
-        }
+    }
+    if (!mbar_wait(&bar, 0, 1u << 22)) {
+        if ((threadIdx.x & 31) == 0) atomicExch(err, 2);
+        return;
+    }
+    const int lane = threadIdx.x & 31, col = lane & 15, half = lane >> 4;
+    const int nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
+    const int x = x0 + col;
+    if (x >= w) return;
+    const long long base = (long long)outer * outer_stride + x;
+    auto at = [&](int q) -> TIn { return tile[q * 16 + col]; };
+    for (int q = 2 * wi + half; q < n; q += 2 * nw) {
+        uint32_t s;
+        uint32_t best = search_line<TIn>(at, q, n, &s);
+        put_line_value<kFinal>(out, base + q * stride, s, best, form);
     }
 }
 
 template <typename TIn, bool kFinal>
-static void line_pass(const TIn* in, void* out, int w, int n, long long stride, long long outer, long long outer_stride,
-                      int form, cudaStream_t st)
+static void line_pass_plain(const TIn* in, void* out, int w, int n, long long stride, long long outer,
+                            long long outer_stride, int form, cudaStream_t st)
 {
     size_t bytes = (size_t)n * 32 * sizeof(TIn);
     const size_t kStageLimit = 200 * 1024;
     dim3 grid((w + 31) / 32, (unsigned)outer);
-    const int threads = 256;
     if (bytes <= kStageLimit) {
         auto kern = k_edt_line<TIn, kFinal, true>;
         if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        kern<<<grid, threads, bytes, st>>>(in, out, w, n, stride, outer_stride, form);
+        kern<<<grid, 256, bytes, st>>>(in, out, w, n, stride, outer_stride, form);
     } else {
-        k_edt_line<TIn, kFinal, false><<<grid, threads, 0, st>>>(in, out, w, n, stride, outer_stride, form);
+        k_edt_line<TIn, kFinal, false><<<grid, 256, 0, st>>>(in, out, w, n, stride, outer_stride, form);
     }
+}
+
+// Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
+// of a w x h x d array.  TMA needs 16-byte row pitches and a tile that fits in
+// shared memory; otherwise the plain form runs.
+template <typename TIn, bool kFinal>
+static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z, int form, int* err, cudaStream_t st)
+{
+    const int n = along_z ? d : h;
+    const long long plane = (long long)w * h;
+    const long long stride = along_z ? plane : w;
+    const long long outer = along_z ? h : d;
+    const long long outer_stride = along_z ? w : plane;
+    const int nbox = (n + 255) / 256;
+    const size_t tile_bytes = (size_t)nbox * 256 * 16 * sizeof(TIn);
+    const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
+    CUtensorMap map;
+    if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {
+        const uint64_t dims[3] = {(uint64_t)w, (uint64_t)h, (uint64_t)d};
+        const uint64_t strides[2] = {(uint64_t)w * sizeof(TIn), (uint64_t)plane * sizeof(TIn)};
+        const uint32_t box[3] = {16u, along_z ? 1u : 256u, along_z ? 256u : 1u};
+        const CUtensorMapDataType type = sizeof(TIn) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+        if (encode_map_3d(&map, in, type, dims, strides, box)) {
+            auto kern = k_edt_line_tma<TIn, kFinal>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+            dim3 grid((w + 15) / 16, (unsigned)outer);
+            kern<<<grid, 512, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err);
+            return;
+        }
+    }
+    line_pass_plain<TIn, kFinal>(in, out, w, n, stride, outer, outer_stride, form, st);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+bool encode_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType type, const uint64_t dims[3],
+                   const uint64_t strides_bytes[2], const uint32_t box[3])
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p) {
+            cudaGetLastError();
+            return false;
+        }
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    const cuuint32_t elem_strides[3] = {1, 1, 1};
+    CUresult r = fn(map, type, 3, const_cast<void*>(base), dims, strides_bytes, box, elem_strides,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 size_t edt_workspace_bytes(int dim, int w, int h, int d)
@@ -245,7 +359,7 @@ size_t edt_workspace_bytes(int dim, int w, int h, int d)
     return b;
 }
 
-void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws,
+void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
                      cudaStream_t st)
 {
     long long rows = (long long)h * (dim == 3 ? d : 1);
@@ -259,17 +373,16 @@ void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, in
     }
     if (dim == 2) {
         ProfScope ps("edt_y_final", st);
-        line_pass<uint16_t, true>(vx, out, w, h, w, 1, 0, form, st);
+        line_pass<uint16_t, true>(vx, out, w, h, 1, 0, form, err, st);
     } else {
         size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
         uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
-        long long plane = (long long)w * h;
         {
             ProfScope ps("edt_y", st);
-            line_pass<uint16_t, false>(vx, ey, w, h, w, d, plane, form, st);   // y lines, outer = z
+            line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st);   // y lines
         }
         ProfScope ps("edt_z_final", st);
-        line_pass<uint32_t, true>(ey, out, w, d, plane, h, w, form, st);   // z lines, outer = y
+        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st);   // z lines
     }
 }
 

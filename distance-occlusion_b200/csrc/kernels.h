@@ -38,7 +38,7 @@ void launch_init_border(int dim, const uint32_t* mask, void* deltas, int w, int 
 
 // k_edt.cu -- mask-driven exact EDT
 size_t edt_workspace_bytes(int dim, int w, int h, int d);
-void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws,
+void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
                      cudaStream_t st);
 // faithful float Felzenszwalb (2D, arbitrary input)
 size_t felz_float_workspace_bytes(int w, int h);

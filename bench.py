@@ -31,7 +31,8 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-W = H = D = 1024
+SIDE = 1024          # volume side; --side changes it (profiling runs use a smaller case)
+W = H = D = SIDE
 SPACING, SEED = 16, 3
 METRIC = "SDF Gvoxels/s (1024^3 value-noise volume, signed Felzenszwalb EDT, mask -> f32)"
 WORKLOAD = "1024^3 value noise (lattice 16, seed 3, threshold 1/2), signed Felzenszwalb SDF, f32 out"
@@ -329,7 +330,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-warmup", type=int, default=1)
+    ap.add_argument("--side", type=int, default=SIDE, help="volume side (1024 = the benchmarked workload)")
     args = ap.parse_args()
+    global W, H, D
+    W = H = D = args.side
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -445,7 +445,7 @@ static dol_status edt_common(int dim, int w, int h, int d, const uint32_t* mask,
     DOL_TRY(check_dims(w, h, d));
     if (form != DOL_EDT_SQUARED && form != DOL_EDT_DIST && form != DOL_EDT_SIGNED)
         return fail(DOL_ERR_INVALID_ARG, "form must be DOL_EDT_SQUARED, DOL_EDT_DIST or DOL_EDT_SIGNED");
-    if (w > 32767 || h > 32767 || d > 32767) return fail(DOL_ERR_UNSUPPORTED, "EDT dimensions are limited to 32767");
+    if (w > 16384 || h > 16384 || d > 16384) return fail(DOL_ERR_UNSUPPORTED, "EDT dimensions are limited to 16384");
     if (h > 65535 || d > 65535) return fail(DOL_ERR_UNSUPPORTED, "EDT grid limit");
     DOL_TRY(check_dev_ptr(mask, "mask"));
     DOL_TRY(check_dev_ptr(out, "out"));

@@ -235,46 +235,96 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
     }
 }
 
-// TMA form: a 16-column x full-line tile arrives in 256-position boxes
-// (cp.async.bulk.tensor, one mbarrier); lanes 0-15 and 16-31 of a warp take
-// two adjacent positions of the 16 columns.  Several CTAs per SM overlap one
-// tile's load with another's search.
-template <typename TIn, bool kFinal>
+// TMA form.  A TX-column x full-line tile arrives in 256-position boxes
+// (cp.async.bulk.tensor, one mbarrier).  It is then split in place into two
+// state-specific arrays: F_s[p] is the cell's value (v or e) when its state is
+// s and 0 otherwise, so for a cell of state s every probe is one load, one
+// multiply-add (or add) and one min -- a cell of the other state at distance k
+// contributes exactly k^2.  The symmetric part of the walk runs without bounds
+// checks; lanes cover TX columns x (32/TX) adjacent positions.
+template <typename TIn>
+__device__ __forceinline__ uint32_t sq_val(TIn v)
+{
+    return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v : (uint32_t)v;
+}
+
+template <typename TIn, bool kFinal, int TX>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
                                                       int along_z, int form, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    TIn* tile = reinterpret_cast<TIn*>(smem_raw);   // [boxes * 256][16]
-    __shared__ __align__(8) uint64_t bar;
-    const int x0 = blockIdx.x * 16;
-    const int outer = blockIdx.y;
     const int nbox = (n + 255) >> 8;
+    const int rows = nbox * 256;
+    TIn* F0 = reinterpret_cast<TIn*>(smem_raw);   // [rows][TX], first the raw tile
+    TIn* F1 = F0 + rows * TX;                      // [rows][TX]
+    __shared__ __align__(8) uint64_t bar;
+    const int x0 = blockIdx.x * TX;
+    const int outer = blockIdx.y;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(&bar, (uint32_t)(nbox * 256 * 16 * sizeof(TIn)));
+        mbar_expect_tx(&bar, (uint32_t)(rows * TX * sizeof(TIn)));
         for (int b = 0; b < nbox; b++) {
             if (along_z)
-                tma_load_3d(tile + b * 256 * 16, &map, x0, outer, b * 256, &bar);
+                tma_load_3d(F0 + b * 256 * TX, &map, x0, outer, b * 256, &bar);
             else
-                tma_load_3d(tile + b * 256 * 16, &map, x0, b * 256, outer, &bar);
+                tma_load_3d(F0 + b * 256 * TX, &map, x0, b * 256, outer, &bar);
         }
     }
     if (!mbar_wait(&bar, 0, 1u << 22)) {
         if ((threadIdx.x & 31) == 0) atomicExch(err, 2);
         return;
     }
-    const int lane = threadIdx.x & 31, col = lane & 15, half = lane >> 4;
+    // split by state: the top bit is the state, the rest the value
+    constexpr int kTop = sizeof(TIn) * 8 - 1;
+    constexpr uint32_t kVal = (1u << kTop) - 1u;
+    for (int i = threadIdx.x; i < n * TX; i += blockDim.x) {
+        uint32_t x = (uint32_t)F0[i];
+        uint32_t v = x & kVal;
+        bool st = (x >> kTop) & 1u;
+        F0[i] = (TIn)(st ? 0u : v);
+        F1[i] = (TIn)(st ? v : 0u);
+    }
+    __syncthreads();
+
+    constexpr int kRowsPerWarp = 32 / TX;
+    const int lane = threadIdx.x & 31, col = lane % TX, sub = lane / TX;
     const int nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
     const int x = x0 + col;
     if (x >= w) return;
     const long long base = (long long)outer * outer_stride + x;
-    auto at = [&](int q) -> TIn { return tile[q * 16 + col]; };
-    for (int q = 2 * wi + half; q < n; q += 2 * nw) {
-        uint32_t s;
-        uint32_t best = search_line<TIn>(at, q, n, &s);
-        put_line_value<kFinal>(out, base + q * stride, s, best, form);
+    // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
+    const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
+    for (int q = kRowsPerWarp * wi + sub; q < n; q += kRowsPerWarp * nw) {
+        const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
+        const TIn* A = (s ? F1 : F0) + col;
+        uint32_t best = sq_val<TIn>(A[q * TX]);
+        const int lmax = q, rmax = n - 1 - q, kmin = min(lmax, rmax);
+        uint32_t k2 = 1, dk = 3;
+        int k = 1;
+        const TIn* pl = A + (q - 1) * TX;
+        const TIn* pr = A + (q + 1) * TX;
+        for (; k <= kmin && k2 < best; k++) {
+            best = min(best, min(sq_val<TIn>(*pl), sq_val<TIn>(*pr)) + k2);
+            pl -= TX;
+            pr += TX;
+            k2 += dk;
+            dk += 2;
+        }
+        for (; k <= lmax && k2 < best; k++) {
+            best = min(best, sq_val<TIn>(*pl) + k2);
+            pl -= TX;
+            k2 += dk;
+            dk += 2;
+        }
+        for (; k <= rmax && k2 < best; k++) {
+            best = min(best, sq_val<TIn>(*pr) + k2);
+            pr += TX;
+            k2 += dk;
+            dk += 2;
+        }
+        put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }
 }
 
@@ -305,19 +355,20 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const long long stride = along_z ? plane : w;
     const long long outer = along_z ? h : d;
     const long long outer_stride = along_z ? w : plane;
+    constexpr int TX = sizeof(TIn) == 2 ? 16 : 8;   // 32-byte box rows either way
     const int nbox = (n + 255) / 256;
-    const size_t tile_bytes = (size_t)nbox * 256 * 16 * sizeof(TIn);
+    const size_t tile_bytes = 2 * (size_t)nbox * 256 * TX * sizeof(TIn);
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
     CUtensorMap map;
     if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {
         const uint64_t dims[3] = {(uint64_t)w, (uint64_t)h, (uint64_t)d};
         const uint64_t strides[2] = {(uint64_t)w * sizeof(TIn), (uint64_t)plane * sizeof(TIn)};
-        const uint32_t box[3] = {16u, along_z ? 1u : 256u, along_z ? 256u : 1u};
+        const uint32_t box[3] = {(uint32_t)TX, along_z ? 1u : 256u, along_z ? 256u : 1u};
         const CUtensorMapDataType type = sizeof(TIn) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
         if (encode_map_3d(&map, in, type, dims, strides, box)) {
-            auto kern = k_edt_line_tma<TIn, kFinal>;
+            auto kern = k_edt_line_tma<TIn, kFinal, TX>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
-            dim3 grid((w + 15) / 16, (unsigned)outer);
+            dim3 grid((w + TX - 1) / TX, (unsigned)outer);
             kern<<<grid, 512, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err);
             return;
         }

@@ -62,6 +62,14 @@ dol_status device_state(DeviceState** out)
             *s.err_host = 0;
             e = cudaHostGetDevicePointer(&s.err_dev, s.err_host, 0);
             if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
+            // keep stream-ordered workspace allocations cached between calls
+            // instead of returning them to the driver at every synchronisation
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            cudaGetLastError();
             s.sms = sms;
             s.ready = true;
         }

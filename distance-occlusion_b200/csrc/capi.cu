@@ -168,6 +168,17 @@ dol_status check_sweep_width(int w)
 
 }  // namespace
 
+int dolk::set_error(int s, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return s;
+}
+
 extern "C" {
 
 int dol_version(void) { return DOL_B200_VERSION; }

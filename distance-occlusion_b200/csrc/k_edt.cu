@@ -437,6 +437,17 @@ void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, in
     }
 }
 
+// 2D mask EDT on caller-provided scratch (w*h uint16), plain loads only: no
+// tensor maps, no bounded waits, nothing allocated.
+void launch_edt_mask_2d_plain(const uint32_t* mask, float* out, int w, int h, int form, uint16_t* scratch, int sms,
+                              cudaStream_t st)
+{
+    long long blocks = ((long long)h * 32 + 255) / 256;
+    long long cap = (long long)sms * 16;
+    k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask, scratch, w, h);
+    line_pass_plain<uint16_t, true>(scratch, out, w, h, w, 1, 0, form, st);
+}
+
 // ------------------------------------------------ faithful float Felzenszwalb ----
 // DOL::Felzenszwalb(w, h, float[]) on arbitrary input: the same 1D lower
 // envelope in the same float operations (DistanceOcclusionLib.cpp:1026-1062),

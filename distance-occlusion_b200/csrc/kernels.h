@@ -21,6 +21,9 @@ private:
     int idx_ = -1;
 };
 
+// records the message returned by dol_last_error() and returns `s`
+int set_error(int s, const char* fmt, ...);
+
 inline uint32_t float_bits(float f)
 {
     uint32_t u;
@@ -40,6 +43,8 @@ void launch_init_border(int dim, const uint32_t* mask, void* deltas, int w, int 
 size_t edt_workspace_bytes(int dim, int w, int h, int d);
 void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
                      cudaStream_t st);
+void launch_edt_mask_2d_plain(const uint32_t* mask, float* out, int w, int h, int form, uint16_t* scratch, int sms,
+                              cudaStream_t st);
 // faithful float Felzenszwalb (2D, arbitrary input)
 size_t felz_float_workspace_bytes(int w, int h);
 void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st);

@@ -142,6 +142,20 @@ DOL_API dol_status dol_edt_mask_2d(int w, int h, const uint32_t* mask, float* ou
 DOL_API dol_status dol_edt_mask_3d(int w, int h, int d, const uint32_t* mask, float* out, int form,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- 2D mask EDT without allocation (no counterpart in the reference) -----------------
+   The same result as dol_edt_mask_2d for callers that cannot allocate device
+   memory when they call: applications that reserve all of their GPU memory up
+   front and forbid allocation afterwards (engines, plugin hosts with their own
+   memory manager), or code that must not risk an allocation failing or
+   stalling mid-frame.  The scratch is a fixed 16 MiB array inside the library
+   that every GPU loading the library holds until the process exits; images are
+   limited to 8,388,608 cells (w*h) and sides to 16384, larger ones return
+   DOL_ERR_UNSUPPORTED.  The first call on a device looks up the array's device
+   address (cudaGetSymbolAddress); make that first call before any stream
+   capture.  All calls share the array, so calls that overlap on the GPU race:
+   serialise them.  mask and out are device memory; nothing is allocated. */
+DOL_API dol_status dol_edt_mask_2d_noalloc(int w, int h, const uint32_t* mask, float* out, int form, void* stream);
+
 /* ---- deltas -> distances ------------------------------------------------------------ */
 /* Dist() (DistanceOcclusionTool.cpp:46-61): out = sqrtf((float)(x*x+y*y[+z*z])) / cw,
    negated where sign_mask (nullable) has the cell's bit (Tool.cpp:1262, :1392) */

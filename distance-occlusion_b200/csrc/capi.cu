@@ -4,8 +4,10 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "dol_b200.h"
 #include "gen.cuh"
@@ -589,6 +591,125 @@ dol_status dol_sdf_3d(int w, int h, int d, const uint32_t* mask, int method, dol
                       void* workspace, size_t workspace_bytes, void* stream)
 {
     return sdf_common(3, w, h, d, mask, method, deltas, dist, workspace, workspace_bytes, stream);
+}
+
+// ---- batched signed fields ------------------------------------------------------------------------
+
+size_t dol_batch_workspace_size(int n)
+{
+    if (n < 1) return 0;
+    return align256((size_t)n * sizeof(dol_batch_item)) + align256((size_t)n * sizeof(int)) + 256;
+}
+
+dol_status dol_batch_prepare(int n, const dol_batch_item* items, void* workspace, size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    if (n < 1 || !items) return fail(DOL_ERR_INVALID_ARG, "need at least one item");
+    if (!workspace) return fail(DOL_ERR_INVALID_ARG, "dol_batch_prepare needs a workspace (dol_batch_workspace_size)");
+    if (workspace_bytes < dol_batch_workspace_size(n)) return fail(DOL_ERR_INVALID_ARG, "workspace too small");
+    DOL_TRY(check_dev_ptr(workspace, "workspace"));
+    std::vector<int> order(n);
+    std::vector<double> work(n);
+    for (int i = 0; i < n; i++) {
+        const dol_batch_item& it = items[i];
+        if (it.w < 1 || it.h < 1 || it.d < 1) return fail(DOL_ERR_INVALID_ARG, "item %d has an empty size", i);
+        if (it.w > 1024) return fail(DOL_ERR_UNSUPPORTED, "item %d: batched rows are limited to 1024 cells", i);
+        if (it.mask_word_offset < 0 || it.delta_byte_offset < 0)
+            return fail(DOL_ERR_INVALID_ARG, "item %d has a negative offset", i);
+        // serial row steps dominate: 2h per image, 2(d-1)*2h per volume, plus the cells themselves
+        work[i] = it.d > 1 ? 4.0 * it.d * it.h + 1e-3 * it.w * it.h * it.d : 2.0 * it.h + 1e-3 * it.w * it.h;
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    char* p = static_cast<char*>(workspace);
+    cudaStream_t st = S(stream);
+    cudaError_t e = cudaMemcpyAsync(p, items, (size_t)n * sizeof(dol_batch_item), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p + align256((size_t)n * sizeof(dol_batch_item)), order.data(), (size_t)n * sizeof(int),
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host order vector ends here
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "batch upload: %s", cudaGetErrorString(e));
+    return DOL_OK;
+}
+
+dol_status dol_batch_run(int n, const uint32_t* masks, void* deltas, float* dist, void* workspace, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    if (n < 1 || !masks || !deltas || !workspace) return fail(DOL_ERR_INVALID_ARG, "missing batch buffer");
+    char* p = static_cast<char*>(workspace);
+    const void* items = p;
+    const int* order = reinterpret_cast<const int*>(p + align256((size_t)n * sizeof(dol_batch_item)));
+    int* counter = reinterpret_cast<int*>(p + align256((size_t)n * sizeof(dol_batch_item)) +
+                                          align256((size_t)n * sizeof(int)));
+    launch_batch_sdf(items, order, n, masks, deltas, dist, counter, S(stream));
+    return launched("batch_sdf");
+}
+
+dol_status dol_batch_sdf(int n, const dol_batch_item* items, const uint32_t* masks, void* deltas, float* dist,
+                         void* workspace, size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dev_ptr(masks, "masks"));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    if (dist) DOL_TRY(check_dev_ptr(dist, "dist"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_batch_workspace_size(n), S(stream)));
+    DOL_TRY(dol_batch_prepare(n, items, ws.ptr, dol_batch_workspace_size(n), stream));
+    return dol_batch_run(n, masks, deltas, dist, ws.ptr, stream);
+}
+
+namespace {
+struct GraphHandle {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+}  // namespace
+
+dol_status dol_batch_graph_create(int n, const uint32_t* masks, void* deltas, float* dist, void* workspace, void** out)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    if (!out) return fail(DOL_ERR_INVALID_ARG, "graph output pointer is NULL");
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail(DOL_ERR_CUDA, "stream");
+    GraphHandle* g = new GraphHandle;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    dol_status s = DOL_OK;
+    if (e == cudaSuccess) {
+        s = dol_batch_run(n, masks, deltas, dist, workspace, st);
+        e = cudaStreamEndCapture(st, &g->graph);
+    }
+    if (e == cudaSuccess && s == DOL_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess || s != DOL_OK) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        cudaGetLastError();
+        return s != DOL_OK ? s : fail(DOL_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    }
+    *out = g;
+    return DOL_OK;
+}
+
+dol_status dol_graph_launch(void* graph, void* stream)
+{
+    if (!graph) return fail(DOL_ERR_INVALID_ARG, "graph is NULL");
+    cudaError_t e = cudaGraphLaunch(static_cast<GraphHandle*>(graph)->exec, S(stream));
+    if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
+    return DOL_OK;
+}
+
+void dol_graph_destroy(void* graph)
+{
+    GraphHandle* g = static_cast<GraphHandle*>(graph);
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
 }
 
 // ---- host-buffer variants --------------------------------------------------------------------------

@@ -252,3 +252,199 @@ DOL_API void dol_gen_shapes_3d_host(int w, int h, int d, int nbox, int nsph, int
 }
 
 }  // extern "C"
+
+// ---- batch of uneven masks: star-shaped polygons and sphere volumes -----------------------
+
+#include <algorithm>
+#include <cmath>
+
+namespace dolk {
+
+// Item geometry for rasterisation.  Polygon vertices are fixed point (1/256
+// cell) so the inside test is integer-exact on host and device.
+struct GenShape {
+    int kind;          // 0 polygon (2D), 1 spheres (3D)
+    int nv;            // polygon vertices / spheres
+    int first;         // index of the first vertex / sphere
+    int pad;
+};
+
+// crossing-number test of the cell centre (x+1/2, y+1/2) against a polygon
+DOL_HD bool polygon_bit(const int* vx, const int* vy, int nv, int x, int y)
+{
+    const long long px = 256LL * x + 128, py = 256LL * y + 128;
+    bool in = false;
+    for (int i = 0, j = nv - 1; i < nv; j = i++) {
+        long long ax = vx[j], ay = vy[j], bx = vx[i], by = vy[i];
+        if ((ay > py) != (by > py)) {
+            // x of the edge at py is ax + (py-ay)(bx-ax)/(by-ay); compare without division
+            long long lhs = (px - ax) * (by - ay), rhs = (py - ay) * (bx - ax);
+            bool left = (by > ay) ? (lhs < rhs) : (lhs > rhs);
+            if (left) in = !in;
+        }
+    }
+    return in;
+}
+
+DOL_HD bool spheres_bit(const int* sp, int n, int x, int y, int z)
+{
+    for (int i = 0; i < n; i++) {
+        long long dx = 2LL * x + 1 - 2LL * sp[4 * i], dy = 2LL * y + 1 - 2LL * sp[4 * i + 1],
+                  dz = 2LL * z + 1 - 2LL * sp[4 * i + 2];
+        long long r2 = 4LL * sp[4 * i + 3] * sp[4 * i + 3];
+        if (dx * dx + dy * dy + dz * dz <= r2) return true;
+    }
+    return false;
+}
+
+__global__ void k_gen_batch(const dol_batch_item* items, const GenShape* shapes, const int* vx, const int* vy,
+                            const int* spheres, uint32_t* masks)
+{
+    const dol_batch_item it = items[blockIdx.x];
+    const GenShape g = shapes[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ws = words_per_row(it.w);
+    const long long rows = (long long)it.h * it.d;
+    uint32_t* m = masks + it.mask_word_offset;
+    for (long long wid = warp; wid < rows * ws; wid += nw) {
+        const long long row = wid / ws;
+        const int k = (int)(wid - row * ws);
+        const int x = 32 * k + lane;
+        bool b = false;
+        if (x < it.w) {
+            if (g.kind == 0)
+                b = polygon_bit(vx + g.first, vy + g.first, g.nv, x, (int)row);
+            else
+                b = spheres_bit(spheres + 4 * g.first, g.nv, x, (int)(row % it.h), (int)(row / it.h));
+        }
+        uint32_t word = __ballot_sync(0xFFFFFFFFu, b);
+        if (lane == 0) m[wid] = word;
+    }
+}
+
+struct BatchSpec {
+    std::vector<dol_batch_item> items;
+    std::vector<GenShape> shapes;
+    std::vector<int> vx, vy, spheres;
+    long long words = 0, delta_bytes = 0, cells = 0;
+};
+
+// The batch geometry from the reference's LCG: n2 images with side
+// log-uniform in [32, 1024] and h = side * U[1, 2], each one star-shaped
+// polygon with 3-12 vertices at sorted random angles and radii U[0.2, 0.45] *
+// side about the centre; then n3 volumes with side uniform in [32, 128], each
+// the union of 8 spheres (centres uniform, radii uniform in [side/8, side/3]).
+static BatchSpec batch_spec(int n2, int n3, uint32_t seed)
+{
+    BatchSpec b;
+    auto next = [&]() { seed = lcg_next(seed); return seed; };
+    auto unit = [&]() { return (double)lcg_scale(next(), 1 << 24) / (double)(1 << 24); };
+    auto pick = [&](int limit) { return lcg_scale(next(), limit); };
+    auto add = [&](int w, int h, int d) {
+        dol_batch_item it{};
+        it.w = w; it.h = h; it.d = d;
+        it.mask_word_offset = b.words;
+        it.delta_byte_offset = b.delta_bytes;
+        it.dist_offset = b.cells;
+        long long cells = (long long)w * h * d;
+        b.words += (long long)words_per_row(w) * h * d;
+        b.delta_bytes += ((cells * (d > 1 ? 6 : 4)) + 15) / 16 * 16;
+        b.cells += cells;
+        b.items.push_back(it);
+    };
+    const double kTwoPi = 6.283185307179586;
+    for (int i = 0; i < n2; i++) {
+        int side = (int)std::floor(32.0 * std::pow(32.0, unit()));
+        if (side > 1024) side = 1024;
+        int h = (int)std::floor(side * (1.0 + unit()));
+        add(side, h, 1);
+        int nv = 3 + pick(10);
+        std::vector<double> ang(nv);
+        for (auto& a : ang) a = unit() * kTwoPi;
+        std::sort(ang.begin(), ang.end());
+        GenShape g{0, nv, (int)b.vx.size(), 0};
+        const double cx = side * 0.5, cy = h * 0.5;
+        for (int v = 0; v < nv; v++) {
+            double r = (0.2 + 0.25 * unit()) * side;
+            b.vx.push_back((int)std::lround(256.0 * (cx + r * std::cos(ang[v]))));
+            b.vy.push_back((int)std::lround(256.0 * (cy + r * std::sin(ang[v]))));
+        }
+        b.shapes.push_back(g);
+    }
+    for (int i = 0; i < n3; i++) {
+        int side = 32 + pick(97);
+        add(side, side, side);
+        GenShape g{1, 8, (int)(b.spheres.size() / 4), 0};
+        for (int s = 0; s < 8; s++) {
+            b.spheres.push_back(pick(side));
+            b.spheres.push_back(pick(side));
+            b.spheres.push_back(pick(side));
+            b.spheres.push_back(side / 8 + pick(side / 3 - side / 8 + 1));
+        }
+        b.shapes.push_back(g);
+    }
+    return b;
+}
+
+}  // namespace dolk
+
+extern "C" {
+
+DOL_API dol_status dol_gen_batch(int n2, int n3, uint32_t seed, dol_batch_item* items, long long* total_mask_words,
+                                 long long* total_delta_bytes, long long* total_cells, uint32_t* masks, void* stream)
+{
+    if (n2 < 0 || n3 < 0) return DOL_ERR_INVALID_ARG;
+    BatchSpec b = batch_spec(n2, n3, seed);
+    if (items) memcpy(items, b.items.data(), b.items.size() * sizeof(dol_batch_item));
+    if (total_mask_words) *total_mask_words = b.words;
+    if (total_delta_bytes) *total_delta_bytes = b.delta_bytes;
+    if (total_cells) *total_cells = b.cells;
+    if (!masks || b.items.empty()) return DOL_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto up = [&](const void* src, size_t bytes, void** dst) {
+        if (bytes == 0) bytes = 4;
+        if (cudaMallocAsync(dst, bytes, st) != cudaSuccess) return false;
+        return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    };
+    void *di = nullptr, *ds = nullptr, *dvx = nullptr, *dvy = nullptr, *dsp = nullptr;
+    int zero[4] = {0, 0, 0, 0};
+    bool ok = up(b.items.data(), b.items.size() * sizeof(dol_batch_item), &di) &&
+              up(b.shapes.data(), b.shapes.size() * sizeof(GenShape), &ds) &&
+              up(b.vx.empty() ? zero : b.vx.data(), b.vx.size() * 4, &dvx) &&
+              up(b.vy.empty() ? zero : b.vy.data(), b.vy.size() * 4, &dvy) &&
+              up(b.spheres.empty() ? zero : b.spheres.data(), b.spheres.size() * 4, &dsp);
+    if (ok) {
+        k_gen_batch<<<(int)b.items.size(), 256, 0, st>>>(static_cast<dol_batch_item*>(di), static_cast<GenShape*>(ds),
+                                                         static_cast<int*>(dvx), static_cast<int*>(dvy),
+                                                         static_cast<int*>(dsp), masks);
+    }
+    for (void* p : {di, ds, dvx, dvy, dsp})
+        if (p) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);   // the host copies of the geometry end with this call
+    return ok && cudaGetLastError() == cudaSuccess ? DOL_OK : DOL_ERR_CUDA;
+}
+
+DOL_API void dol_gen_batch_host(int n2, int n3, uint32_t seed, uint32_t* masks)
+{
+    BatchSpec b = batch_spec(n2, n3, seed);
+    for (size_t i = 0; i < b.items.size(); i++) {
+        const dol_batch_item& it = b.items[i];
+        const GenShape& g = b.shapes[i];
+        const int ws = words_per_row(it.w);
+        uint32_t* m = masks + it.mask_word_offset;
+        for (long long row = 0; row < (long long)it.h * it.d; row++)
+            for (int k = 0; k < ws; k++) {
+                uint32_t word = 0;
+                for (int bit = 0; bit < 32 && 32 * k + bit < it.w; bit++) {
+                    int x = 32 * k + bit;
+                    bool in = g.kind == 0 ? polygon_bit(b.vx.data() + g.first, b.vy.data() + g.first, g.nv, x, (int)row)
+                                          : spheres_bit(b.spheres.data() + 4 * g.first, g.nv, x, (int)(row % it.h),
+                                                        (int)(row / it.h));
+                    if (in) word |= 1u << bit;
+                }
+                m[row * ws + k] = word;
+            }
+    }
+}
+
+}  // extern "C"

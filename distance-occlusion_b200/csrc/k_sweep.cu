@@ -45,10 +45,11 @@ __device__ __forceinline__ C3 cell_load_cg(const int16_t* p, long long i)
 
 // ------------------------------------------------------------ Danielsson 2D ----
 
+// One CTA runs the whole 2D Danielsson of one image (used by the single-image
+// kernel and by the batched kernel).
 template <int S>
-__global__ void __launch_bounds__(512) k_danielsson2(uint32_t* __restrict__ dl, int w, int h, int cw)
+__device__ __forceinline__ void danielsson2_cta(uint32_t* __restrict__ dl, int w, int h, int cw, ScanShared<C2>& sh)
 {
-    __shared__ ScanShared<C2> sh;
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
     const int n = t < nseg ? min(S, w - t * S) : 0;
@@ -84,15 +85,22 @@ __global__ void __launch_bounds__(512) k_danielsson2(uint32_t* __restrict__ dl, 
     }
 }
 
+template <int S>
+__global__ void __launch_bounds__(512) k_danielsson2(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    __shared__ ScanShared<C2> sh;
+    danielsson2_cta<S>(dl, w, h, cw, sh);
+}
+
 // ------------------------------------------------------------ Danielsson 3D ----
 // Slices 1..d-1 then d-2..0 (:2355-2393); each slice takes the neighbouring
 // slice's cell with the z offset, then runs the 2D sweeps over its rows
 // (:2264-2345).  The z pull is folded into the first load of each row.
 
 template <int S>
-__global__ void __launch_bounds__(512) k_danielsson3(int16_t* __restrict__ dl, int w, int h, int d, int cw)
+__device__ __forceinline__ void danielsson3_cta(int16_t* __restrict__ dl, int w, int h, int d, int cw,
+                                                ScanShared<C3>& sh)
 {
-    __shared__ ScanShared<C3> sh;
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
     const int n = t < nseg ? min(S, w - t * S) : 0;
@@ -137,6 +145,13 @@ __global__ void __launch_bounds__(512) k_danielsson3(int16_t* __restrict__ dl, i
             }
         }
     }
+}
+
+template <int S>
+__global__ void __launch_bounds__(512) k_danielsson3(int16_t* __restrict__ dl, int w, int h, int d, int cw)
+{
+    __shared__ ScanShared<C3> sh;
+    danielsson3_cta<S>(dl, w, h, d, cw, sh);
 }
 
 // ------------------------------------------------------------- FastSweep 2D ----
@@ -399,6 +414,117 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
         default: break;
     }
 #undef DOL_FS3_CASE
+}
+
+}  // namespace dolk
+
+// ------------------------------------------------------------- batched SDF ----
+// Thousands of independent masks and volumes in one persistent launch: each
+// CTA pulls the next item (largest first) from an atomic counter and runs the
+// whole signed pipeline on it -- border initialisation, Danielsson with cw = 2,
+// signed distances -- with the same per-CTA code as the single-item kernels,
+// so every item's output is bit-identical to a per-item call.
+#include "border.cuh"
+
+namespace dolk {
+
+struct BatchItemDev {
+    int w, h, d, pad;
+    long long mask_off;    // words
+    long long delta_off;   // bytes
+    long long dist_off;    // floats, < 0: none
+};
+
+__device__ __forceinline__ void border2_cta(const uint32_t* mask, uint32_t* dl, int w, int h)
+{
+    const int ws = words_per_row(w);
+    for (long long wid = threadIdx.x; wid < (long long)ws * h; wid += blockDim.x) {
+        const int y = (int)(wid / ws), k = (int)(wid - (long long)y * ws);
+        Planes2 p = border2_word(w, h, mask, y, k);
+        const int n = min(32, w - 32 * k);
+        uint32_t* row = dl + (long long)y * w + 32 * k;
+        for (int b = 0; b < n; b++) row[b] = pack2(decode2(p, b));
+    }
+}
+
+__device__ __forceinline__ void border3_cta(const uint32_t* mask, int16_t* dl, int w, int h, int d)
+{
+    const int ws = words_per_row(w);
+    const long long words = (long long)ws * h * d;
+    for (long long wid = threadIdx.x; wid < words; wid += blockDim.x) {
+        const long long row = wid / ws;
+        const int k = (int)(wid - row * ws);
+        const int z = (int)(row / h), y = (int)(row - (long long)z * h);
+        Planes3 p = border3_word(w, h, d, mask, z, y, k);
+        const int n = min(32, w - 32 * k);
+        for (int b = 0; b < n; b++) cell_store(dl, row * w + 32 * k + b, decode3(p, b));
+    }
+}
+
+template <class Cell, class P>
+__device__ __forceinline__ void signed_dist_cta(const uint32_t* mask, const P* dl, float* out, int w, long long rows)
+{
+    const int ws = words_per_row(w);
+    for (long long i = threadIdx.x; i < rows * w; i += blockDim.x) {
+        const long long row = i / w;
+        const int x = (int)(i - row * w);
+        float r = __fdiv_rn(sqrtf((float)len(cell_load(dl, i))), 2.0f);
+        if ((mask[row * ws + (x >> 5)] >> (x & 31)) & 1u) r = -r;
+        out[i] = r;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restrict__ items, const int* __restrict__ order,
+                                                   int n, const uint32_t* __restrict__ masks,
+                                                   unsigned char* __restrict__ deltas, float* __restrict__ dist,
+                                                   int* __restrict__ counter)
+{
+    __shared__ ScanShared<C3> sh3;   // the larger of the two; the 2D engine reuses its storage
+    __shared__ int s_item;
+    ScanShared<C2>& sh2 = *reinterpret_cast<ScanShared<C2>*>(&sh3);
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= n) break;
+        const BatchItemDev b = items[order[it]];
+        const uint32_t* m = masks + b.mask_off;
+        if (b.d <= 1) {
+            uint32_t* dl = reinterpret_cast<uint32_t*>(deltas + b.delta_off);
+            border2_cta(m, dl, b.w, b.h);
+            __syncthreads();
+            danielsson2_cta<S>(dl, b.w, b.h, 2, sh2);
+            __syncthreads();
+            if (dist && b.dist_off >= 0) signed_dist_cta<C2>(m, dl, dist + b.dist_off, b.w, b.h);
+        } else {
+            int16_t* dl = reinterpret_cast<int16_t*>(deltas + b.delta_off);
+            border3_cta(m, dl, b.w, b.h, b.d);
+            __syncthreads();
+            danielsson3_cta<S>(dl, b.w, b.h, b.d, 2, sh3);
+            __syncthreads();
+            if (dist && b.dist_off >= 0) signed_dist_cta<C3>(m, dl, dist + b.dist_off, b.w, (long long)b.h * b.d);
+        }
+        __syncthreads();
+    }
+}
+
+static_assert(sizeof(BatchItemDev) == 40, "batch item layout (dol_batch_item)");
+
+void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t* masks, void* deltas, float* dist,
+                      int* counter, cudaStream_t st)
+{
+    ProfScope ps("batch_sdf", st);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_sdf<4>, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+    int grid = per_sm * g_num_sms;
+    if (grid > n) grid = n;
+    if (grid < 1) grid = 1;
+    cudaMemsetAsync(counter, 0, sizeof(int), st);
+    k_batch_sdf<4><<<grid, 256, 0, st>>>(static_cast<const BatchItemDev*>(items), order, n, masks,
+                                         static_cast<unsigned char*>(deltas), dist, counter);
 }
 
 }  // namespace dolk

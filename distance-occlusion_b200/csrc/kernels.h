@@ -59,6 +59,9 @@ void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* 
 void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st);
 void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st);
 size_t fastsweep3_workspace_bytes(int w, int h, int d);
+// batched signed Danielsson; items: device array of dol_batch_item (40 bytes)
+void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t* masks, void* deltas, float* dist,
+                      int* counter, cudaStream_t st);
 void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, int* err, cudaStream_t st);
 
 }  // namespace dolk

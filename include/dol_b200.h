@@ -181,6 +181,39 @@ DOL_API dol_status dol_sdf_3d_host(int w, int h, int d, const uint32_t* mask, in
 /* Mask-driven EDT with host buffers (DOL_EDT_* form) */
 DOL_API dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float* out, int form);
 
+/* ---- batched signed fields (no reference counterpart) ----------------------------------
+   Many independent images and volumes of different sizes, each run through
+   the signed border pipeline of dol_sdf_2d/3d with Danielsson (border init,
+   cw = 2 propagation, signed distances), in ONE persistent launch: each CTA
+   takes the next item, largest first, from an atomic counter.  Every item's
+   deltas and distances are bit-identical to a per-item dol_sdf_* call.
+   Items: d = 1 for an image; w <= 1024.  masks, deltas, dist are single
+   device buffers; each item gives its offsets into them (dist_offset < 0: no
+   distances for that item).  dol_batch_prepare uploads and orders the items
+   into the workspace once; dol_batch_run only launches (and may be captured
+   into a graph, which dol_batch_graph_create does). */
+typedef struct dol_batch_item {
+    int w, h, d;                    /* d = 1 for an image                         */
+    int reserved;                   /* 0                                          */
+    long long mask_word_offset;     /* into masks (uint32 words)                  */
+    long long delta_byte_offset;    /* into deltas (4-byte cells 2D, 6-byte 3D)   */
+    long long dist_offset;          /* into dist (floats); < 0: no distances      */
+} dol_batch_item;
+
+DOL_API size_t     dol_batch_workspace_size(int n_items);
+DOL_API dol_status dol_batch_prepare(int n_items, const dol_batch_item* host_items, void* workspace,
+                                     size_t workspace_bytes, void* stream);
+DOL_API dol_status dol_batch_run(int n_items, const uint32_t* masks, void* deltas, float* dist, void* workspace,
+                                 void* stream);
+DOL_API dol_status dol_batch_sdf(int n_items, const dol_batch_item* host_items, const uint32_t* masks, void* deltas,
+                                 float* dist, void* workspace, size_t workspace_bytes, void* stream);
+/* CUDA graph of dol_batch_run on a prepared workspace; launch it with
+   dol_graph_launch, release it with dol_graph_destroy */
+DOL_API dol_status dol_batch_graph_create(int n_items, const uint32_t* masks, void* deltas, float* dist,
+                                          void* workspace, void** graph);
+DOL_API dol_status dol_graph_launch(void* graph, void* stream);
+DOL_API void       dol_graph_destroy(void* graph);
+
 /* ---- synthetic inputs (no reference counterpart) --------------------------------------
    Integer-exact, so host and device give the same bits.  Value noise: lattice
    spacing `spacing`, lattice values in [0,65536) from the reference's LCG drawn
@@ -193,6 +226,15 @@ DOL_API dol_status dol_gen_shapes_3d(int w, int h, int d, int nbox, int nsph, in
                                      uint32_t* mask, void* stream);
 DOL_API void       dol_gen_shapes_3d_host(int w, int h, int d, int nbox, int nsph, int smin, int smax, uint32_t seed,
                                           uint32_t* host_mask);
+
+/* Batch of n2 images (side log-uniform in [32,1024], h = side * U[1,2], one
+   star-shaped polygon of 3-12 vertices each, radii U[0.2,0.45]*side) then n3
+   volumes (side U[32,128], union of 8 spheres), geometry from the LCG.
+   Fills items (n2+n3 entries, offsets packed in order) and the totals; with a
+   non-NULL device `masks` (total_mask_words words) also rasterises them. */
+DOL_API dol_status dol_gen_batch(int n2, int n3, uint32_t seed, dol_batch_item* items, long long* total_mask_words,
+                                 long long* total_delta_bytes, long long* total_cells, uint32_t* masks, void* stream);
+DOL_API void       dol_gen_batch_host(int n2, int n3, uint32_t seed, uint32_t* host_masks);
 
 /* ---- launch profiler (no reference counterpart) -----------------------------------------
    Between begin and end every kernel the library launches is bracketed by CUDA

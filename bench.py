@@ -183,6 +183,159 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- per-configuration lines ----
+
+def _ev_ms(torch, fn, reps=1):
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        fn()
+    b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def measure_configs(dol, torch, cpu=True, big=True):
+    """Secondary measurements on the other workloads: the 2D default
+    (1024^2, 100 points, seed 1, unsigned Danielsson), the 256^3 signed volume
+    (32 boxes + 32 spheres, sizes 4-40, seed 7) with every method, the batch
+    of 4096 uneven masks + 64 volumes (batched launch vs per-item loop), and
+    Danielsson on the 1024^3 noise volume.  GPU times are CUDA events on
+    device-resident data; CPU times are the reference library (oracle/_ref),
+    one thread, on the same inputs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    L = dol.lib()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    res = {}
+    ref = O.ref() if cpu else None
+
+    # configuration 1
+    dims = (1024, 1024)
+    m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+    md = torch.from_numpy(m.view(np.int32)).cuda()
+    dl = dol.init_deltas(md, dims)
+    base = dl.clone()
+    dol.danielsson(dl, dims, 1)
+    torch.cuda.synchronize()
+
+    def run_c1():
+        dl.copy_(base)
+        dol.danielsson(dl, dims, 1)
+    t_copy = _ev_ms(torch, lambda: dl.copy_(base), 5)
+    t = _ev_ms(torch, run_c1, 5) - t_copy
+    c1 = {"workload": "1024^2, 100 points (seed 1), unsigned Danielsson deltas", "gpu_ms": t,
+          "gpu_mcells_per_s": 1024 * 1024 / t / 1e3}
+    if ref is not None:
+        ini = O.init_deltas(m, dims, use_ref=True)
+        t0 = time.perf_counter()
+        O.propagate("danielsson", ini, dims, 1, use_ref=True)
+        c1["cpu_ref_ms"] = (time.perf_counter() - t0) * 1e3
+    res["danielsson_2d_1024"] = c1
+
+    # configuration 2: 256^3 signed, every method
+    n = 256
+    dims = (n, n, n)
+    md = torch.empty(dol.mask_words(*dims), dtype=torch.int32, device="cuda")
+    dol.check(L.dol_gen_shapes_3d(n, n, n, 32, 32, 4, 40, C.c_uint32(7), C.c_void_p(md.data_ptr()), sp))
+    occ = float(np.unpackbits(md.cpu().numpy().view(np.uint8)).sum()) / n ** 3
+    c2 = {"workload": "256^3, 32 boxes + 32 spheres (4-40, seed 7), signed", "occupancy": occ}
+    bor = dol.init_border(md, dims)
+    c2["border_init_ms"] = _ev_ms(torch, lambda: dol.init_border(md, dims, out=bor), 3)
+    work = bor.clone()
+    for meth in ("danielsson", "fastsweep", "jumpflood"):
+        def run(meth=meth):
+            work.copy_(bor)
+            dol.propagate(meth, work, dims, 2)
+        run()
+        torch.cuda.synchronize()
+        c2[f"{meth}_ms"] = _ev_ms(torch, run, 2) - _ev_ms(torch, lambda: work.copy_(bor), 2)
+    out = dol.empty_field(dims)
+    c2["felzenszwalb_sdf_ms"] = _ev_ms(torch, lambda: dol.edt_mask(md, dims, dol.EDT_SIGNED, out=out), 3)
+    if ref is not None:
+        mh = md.cpu().numpy().view(np.uint32)
+        b0 = O.border_init(mh, dims, use_ref=True)
+        for meth in ("danielsson", "fastsweep"):
+            t0 = time.perf_counter()
+            O.propagate(meth, b0, dims, 2, use_ref=True)
+            c2[f"cpu_ref_{meth}_ms"] = (time.perf_counter() - t0) * 1e3
+    res["signed_256"] = c2
+
+    # configuration 4: batch
+    n2, n3 = 4096, 64
+    nitems = n2 + n3
+    Item = _batch_item_type()
+    items = (Item * nitems)()
+    tw, tb, tc = C.c_longlong(), C.c_longlong(), C.c_longlong()
+    dol.check(L.dol_gen_batch(n2, n3, C.c_uint32(4), items, C.byref(tw), C.byref(tb), C.byref(tc), None, None))
+    bm = torch.empty(tw.value, dtype=torch.int32, device="cuda")
+    dol.check(L.dol_gen_batch(n2, n3, C.c_uint32(4), items, None, None, None, C.c_void_p(bm.data_ptr()), sp))
+    bd = torch.empty(tb.value, dtype=torch.uint8, device="cuda")
+    bf = torch.empty(tc.value, dtype=torch.float32, device="cuda")
+    wsb = L.dol_batch_workspace_size(nitems)
+    bws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    dol.check(L.dol_batch_prepare(nitems, items, C.c_void_p(bws.data_ptr()), C.c_size_t(wsb), sp))
+    g = C.c_void_p()
+    dol.check(L.dol_batch_graph_create(nitems, C.c_void_p(bm.data_ptr()), C.c_void_p(bd.data_ptr()),
+                                       C.c_void_p(bf.data_ptr()), C.c_void_p(bws.data_ptr()), C.byref(g)))
+    dol.check(L.dol_graph_launch(g, sp))
+    torch.cuda.synchronize()
+    t_batch = _ev_ms(torch, lambda: dol.check(L.dol_graph_launch(g, sp)), 3)
+    L.dol_graph_destroy(g)
+    # per-item loop: one dol_sdf_* call per item on the same buffers, over a sample of items
+    sample = list(range(0, nitems, max(1, nitems // 256)))
+    ws_loop = torch.empty(64 << 20, dtype=torch.uint8, device="cuda")
+
+    def loop():
+        for i in sample:
+            it = items[i]
+            mptr = C.c_void_p(bm.data_ptr() + 4 * it.mask_word_offset)
+            dptr = C.c_void_p(bd.data_ptr() + it.delta_byte_offset)
+            fptr = C.c_void_p(bf.data_ptr() + 4 * it.dist_offset)
+            if it.d == 1:
+                dol.check(L.dol_sdf_2d(it.w, it.h, mptr, dol.DANIELSSON, dptr, fptr, C.c_void_p(ws_loop.data_ptr()),
+                                       C.c_size_t(64 << 20), sp))
+            else:
+                dol.check(L.dol_sdf_3d(it.w, it.h, it.d, mptr, dol.DANIELSSON, dptr, fptr,
+                                       C.c_void_p(ws_loop.data_ptr()), C.c_size_t(64 << 20), sp))
+    loop()
+    torch.cuda.synchronize()
+    t_loop = _ev_ms(torch, loop, 1)
+    cells = tc.value
+    res["batch_4096_64"] = {
+        "workload": "4096 polygon masks (side 32-1024, aspect 1-2) + 64 sphere volumes (32-128), signed Danielsson",
+        "items": nitems, "cells": cells, "batched_ms": t_batch, "batched_masks_per_s": nitems / t_batch * 1e3,
+        "looped_sample_items": len(sample), "looped_ms": t_loop,
+        "looped_masks_per_s": len(sample) / t_loop * 1e3,
+        "batched_over_looped": (nitems / t_batch) / (len(sample) / t_loop),
+        "path": "batched: one persistent launch replayed from a CUDA graph; looped: dol_sdf_* per item"}
+
+    # configuration 3, Danielsson on the 1024^3 noise volume (serial in z and y: seconds)
+    if big:
+        side = 1024
+        mdv = torch.empty(dol.mask_words(side, side, side), dtype=torch.int32, device="cuda")
+        dol.check(L.dol_gen_value_noise_3d(side, side, side, SPACING, C.c_uint32(SEED), C.c_void_p(mdv.data_ptr()), sp))
+        dv = torch.empty((side, side, side, 3), dtype=torch.int16, device="cuda")
+        dol.init_border(mdv, (side,) * 3, out=dv)
+        torch.cuda.synchronize()
+        t = _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)
+        res["danielsson_3d_1024"] = {"workload": "1024^3 value noise, signed Danielsson deltas (cw=2)", "gpu_ms": t,
+                                     "gvox_per_s": side ** 3 / t / 1e6,
+                                     "note": "serial in z and y (each slice needs the previous one after its full "
+                                             "2D sweep): one CTA, latency-bound"}
+        del dv, mdv
+    return res
+
+
+def _batch_item_type():
+    class Item(C.Structure):
+        _fields_ = [("w", C.c_int), ("h", C.c_int), ("d", C.c_int), ("reserved", C.c_int),
+                    ("mask_word_offset", C.c_longlong), ("delta_byte_offset", C.c_longlong),
+                    ("dist_offset", C.c_longlong)]
+    return Item
+
+
 # ---------------------------------------------------------------------- our arm ----
 
 def run_dol(args):
@@ -304,6 +457,11 @@ def run_dol(args):
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_reference_sample(side=args.cpu_side, target_s=args.cpu_seconds)
+    configs = None
+    if not args.no_configs:
+        del work
+        torch.cuda.empty_cache()
+        configs = measure_configs(dol, torch, cpu=(ws == 1 and not args.no_cpu), big=not args.no_big)
     line = {
         "metric": METRIC, "value": value, "unit": "Gvoxels/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -312,6 +470,7 @@ def run_dol(args):
                    "l2": "inputs and outputs > L2 (128 MiB mask in, 4 GiB field out); no flush needed"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "gpu_launches": 3 * args.steps,
+        "configs": configs,
     }
     print(json.dumps(line), flush=True)
     if pg:
@@ -331,6 +490,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--side", type=int, default=SIDE, help="volume side (1024 = the benchmarked workload)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration measurements")
+    ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
     args = ap.parse_args()
     global W, H, D
     W = H = D = args.side

@@ -196,7 +196,7 @@ def _ev_ms(torch, fn, reps=1):
     return a.elapsed_time(b) / reps
 
 
-def measure_configs(dol, torch, cpu=True, big=True):
+def measure_configs(dol, torch, cpu=True, big=True, only=None):
     """Secondary measurements on the other workloads: the 2D default
     (1024^2, 100 points, seed 1, unsigned Danielsson), the 256^3 signed volume
     (32 boxes + 32 spheres, sizes 4-40, seed 7) with every method, the batch
@@ -210,9 +210,20 @@ def measure_configs(dol, torch, cpu=True, big=True):
     sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     res = {}
     ref = O.ref() if cpu else None
+    want = (lambda key: only is None or key in only)
 
-    # configuration 1
-    dims = (1024, 1024)
+    if want("c1"):
+        _config1(dol, torch, O, ref, res, (1024, 1024))
+    if want("c2"):
+        _config2(dol, torch, O, ref, res, L, sp)
+    if want("c4"):
+        _config4(dol, torch, res, L, sp)
+    if big and want("c3"):
+        _config3(dol, torch, res, L, sp)
+    return res
+
+
+def _config1(dol, torch, O, ref, res, dims):
     m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
     md = torch.from_numpy(m.view(np.int32)).cuda()
     dl = dol.init_deltas(md, dims)
@@ -234,7 +245,8 @@ def measure_configs(dol, torch, cpu=True, big=True):
         c1["cpu_ref_ms"] = (time.perf_counter() - t0) * 1e3
     res["danielsson_2d_1024"] = c1
 
-    # configuration 2: 256^3 signed, every method
+
+def _config2(dol, torch, O, ref, res, L, sp):
     n = 256
     dims = (n, n, n)
     md = torch.empty(dol.mask_words(*dims), dtype=torch.int32, device="cuda")
@@ -262,7 +274,8 @@ def measure_configs(dol, torch, cpu=True, big=True):
             c2[f"cpu_ref_{meth}_ms"] = (time.perf_counter() - t0) * 1e3
     res["signed_256"] = c2
 
-    # configuration 4: batch
+
+def _config4(dol, torch, res, L, sp):
     n2, n3 = 4096, 64
     nitems = n2 + n3
     Item = _batch_item_type()
@@ -311,8 +324,9 @@ def measure_configs(dol, torch, cpu=True, big=True):
         "batched_over_looped": (nitems / t_batch) / (len(sample) / t_loop),
         "path": "batched: one persistent launch replayed from a CUDA graph; looped: dol_sdf_* per item"}
 
-    # configuration 3, Danielsson on the 1024^3 noise volume (serial in z and y: seconds)
-    if big:
+
+def _config3(dol, torch, res, L, sp):
+    if True:
         side = 1024
         mdv = torch.empty(dol.mask_words(side, side, side), dtype=torch.int32, device="cuda")
         dol.check(L.dol_gen_value_noise_3d(side, side, side, SPACING, C.c_uint32(SEED), C.c_void_p(mdv.data_ptr()), sp))
@@ -325,7 +339,6 @@ def measure_configs(dol, torch, cpu=True, big=True):
                                      "note": "serial in z and y (each slice needs the previous one after its full "
                                              "2D sweep): one CTA, latency-bound"}
         del dv, mdv
-    return res
 
 
 def _batch_item_type():
@@ -492,11 +505,18 @@ def main():
     ap.add_argument("--side", type=int, default=SIDE, help="volume side (1024 = the benchmarked workload)")
     ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration measurements")
     ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
+    ap.add_argument("--only", default=None,
+                    help="comma list of c1,c2,c3,c4: run only these per-configuration measurements (no headline)")
     args = ap.parse_args()
     global W, H, D
     W = H = D = args.side
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        import torch
+        dol = load_dol()
+        print(json.dumps(measure_configs(dol, torch, cpu=not args.no_cpu, big=True,
+                                         only=set(args.only.split(",")))), flush=True)
     else:
         run_dol(args)
 

@@ -66,7 +66,8 @@ def lib():
         L.dol_status_string.restype = C.c_char_p
         for name in ("dol_mask_words", "dol_jumpflood_2d_workspace_size", "dol_jumpflood_3d_workspace_size",
                      "dol_fastsweep_3d_workspace_size", "dol_felzenszwalb_2d_workspace_size",
-                     "dol_edt_mask_2d_workspace_size", "dol_edt_mask_3d_workspace_size", "dol_sdf_workspace_size"):
+                     "dol_edt_mask_2d_workspace_size", "dol_edt_mask_3d_workspace_size", "dol_sdf_workspace_size",
+                     "dol_batch_workspace_size", "dol_sites_backward_workspace_size"):
             getattr(L, name).restype = C.c_size_t
         _lib = L
     return _lib
@@ -304,3 +305,76 @@ def sdf_host(mask_np, dims, method="danielsson", want_deltas=True, want_dist=Tru
         check(lib().dol_sdf_3d_host(*_ints(*dims), pm, C.c_int(m), pd, pf))
     del cells
     return dl, df
+
+
+# ---- float sites ---------------------------------------------------------------------------------
+
+def gen_sites(n, dims, seed):
+    """n float sites uniform in continuous cell coordinates, from the reference's
+    LCG (24-bit fractions, drawn x, y[, z] per site); float32 array (n, dim)."""
+    import numpy as np
+    dims = _dims(dims)
+    out = np.empty((n, len(dims)), dtype=np.float32)
+    s = seed & 0xFFFFFFFF
+    for i in range(n):
+        for a, extent in enumerate(dims):
+            s = (s * 1103515245 + 12345) & 0xFFFFFFFF
+            frac = ((s * (1 << 24)) >> 32) / float(1 << 24)
+            out[i, a] = np.float32(frac * extent)
+    return out
+
+
+def sites_forward(sites, dims, method="danielsson", stream=None):
+    """Distances from every cell centre to its owning site, through a delta
+    method run on the cells that hold the sites.  Returns (dist, owner, deltas)."""
+    torch = _torch()
+    dims = _dims(dims)
+    dim = len(dims)
+    w, h = dims[0], dims[1]
+    d = dims[2] if dim == 3 else 1
+    n = int(sites.shape[0])
+    mask = torch.empty(mask_words(w, h, d), dtype=torch.int32, device=sites.device)
+    cell_site = torch.empty(tuple(reversed(dims)), dtype=torch.int32, device=sites.device)
+    check(lib().dol_sites_seed(*_ints(dim, w, h, d, n), _ptr(sites), _ptr(mask), _ptr(cell_site), _stream(stream)))
+    deltas = init_deltas(mask, dims, stream=stream)
+    propagate(method, deltas, dims, 1, stream=stream)
+    owner = torch.empty(tuple(reversed(dims)), dtype=torch.int32, device=sites.device)
+    dist = torch.empty(tuple(reversed(dims)), dtype=torch.float32, device=sites.device)
+    check(lib().dol_sites_forward(*_ints(dim, w, h, d, n), _ptr(deltas), _ptr(cell_site), _ptr(sites), _ptr(owner),
+                                  _ptr(dist), _stream(stream)))
+    return dist, owner, deltas
+
+
+def sites_backward(owner, sites, grad_dist, dims, stream=None):
+    """dL/dsites for dL/ddist, with the owner assignment held fixed."""
+    torch = _torch()
+    dims = _dims(dims)
+    dim = len(dims)
+    w, h = dims[0], dims[1]
+    d = dims[2] if dim == 3 else 1
+    n = int(sites.shape[0])
+    grad = torch.empty_like(sites)
+    check(lib().dol_sites_backward(*_ints(dim, w, h, d, n), _ptr(owner), _ptr(sites), _ptr(grad_dist), _ptr(grad),
+                                   None, C.c_size_t(0), _stream(stream)))
+    return grad
+
+
+def site_distance_function():
+    """torch.autograd.Function over sites_forward / sites_backward (used for gradient checks)."""
+    torch = _torch()
+
+    class SiteDistance(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, sites, dims, method):
+            s = sites.detach().contiguous()
+            dist, owner, _ = sites_forward(s, dims, method)
+            ctx.save_for_backward(s, owner)
+            ctx.dims = dims
+            return dist
+
+        @staticmethod
+        def backward(ctx, grad):
+            s, owner = ctx.saved_tensors
+            return sites_backward(owner, s, grad.contiguous(), ctx.dims), None, None
+
+    return SiteDistance

@@ -712,6 +712,66 @@ void dol_graph_destroy(void* graph)
     delete g;
 }
 
+// ---- float sites ---------------------------------------------------------------------------------
+
+static dol_status sites_common(int dim, int w, int h, int d, int n)
+{
+    if (dim != 2 && dim != 3) return fail(DOL_ERR_INVALID_ARG, "dim must be 2 or 3");
+    if (dim == 2 && d != 1) return fail(DOL_ERR_INVALID_ARG, "2D site grids have d = 1");
+    DOL_TRY(check_dims(w, h, d));
+    if (n < 0) return fail(DOL_ERR_INVALID_ARG, "negative site count");
+    return DOL_OK;
+}
+
+dol_status dol_sites_seed(int dim, int w, int h, int d, int n, const float* sites, uint32_t* mask, int* cell_site,
+                          void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(sites_common(dim, w, h, d, n));
+    if (n > 0) DOL_TRY(check_dev_ptr(sites, "sites"));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(cell_site, "cell_site"));
+    launch_sites_seed(dim, w, h, d, n, sites, mask, cell_site, S(stream));
+    return launched("sites_seed");
+}
+
+dol_status dol_sites_forward(int dim, int w, int h, int d, int n, const void* deltas, const int* cell_site,
+                             const float* sites, int* owner, float* dist, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(sites_common(dim, w, h, d, n));
+    DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    DOL_TRY(check_dev_ptr(cell_site, "cell_site"));
+    if (n > 0) DOL_TRY(check_dev_ptr(sites, "sites"));
+    DOL_TRY(check_dev_ptr(owner, "owner"));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    launch_sites_forward(dim, w, h, d, n, deltas, cell_site, sites, owner, dist, S(stream));
+    return launched("sites_forward");
+}
+
+size_t dol_sites_backward_workspace_size(int dim, int n) { return n > 0 ? (size_t)n * dim * sizeof(double) : 0; }
+
+dol_status dol_sites_backward(int dim, int w, int h, int d, int n, const int* owner, const float* sites,
+                              const float* grad_dist, float* grad_sites, void* workspace, size_t workspace_bytes,
+                              void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(sites_common(dim, w, h, d, n));
+    if (n == 0) return DOL_OK;
+    DOL_TRY(check_dev_ptr(owner, "owner"));
+    DOL_TRY(check_dev_ptr(sites, "sites"));
+    DOL_TRY(check_dev_ptr(grad_dist, "grad_dist"));
+    DOL_TRY(check_dev_ptr(grad_sites, "grad_sites"));
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_sites_backward_workspace_size(dim, n), S(stream)));
+    launch_sites_backward(dim, w, h, d, n, owner, sites, grad_dist, static_cast<double*>(ws.ptr), grad_sites,
+                          S(stream));
+    return launched("sites_backward");
+}
+
 // ---- host-buffer variants --------------------------------------------------------------------------
 
 namespace {

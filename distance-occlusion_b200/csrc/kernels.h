@@ -64,4 +64,12 @@ void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t
                       int* counter, cudaStream_t st);
 void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, int* err, cudaStream_t st);
 
+// k_sites.cu
+void launch_sites_seed(int dim, int w, int h, int d, int n, const float* sites, uint32_t* mask, int* cell_site,
+                       cudaStream_t st);
+void launch_sites_forward(int dim, int w, int h, int d, int n, const void* deltas, const int* cell_site,
+                          const float* sites, int* owner, float* dist, cudaStream_t st);
+void launch_sites_backward(int dim, int w, int h, int d, int n, const int* owner, const float* sites,
+                           const float* grad_dist, double* acc, float* grad_sites, cudaStream_t st);
+
 }  // namespace dolk

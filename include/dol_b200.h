@@ -214,6 +214,27 @@ DOL_API dol_status dol_batch_graph_create(int n_items, const uint32_t* masks, vo
 DOL_API dol_status dol_graph_launch(void* graph, void* stream);
 DOL_API void       dol_graph_destroy(void* graph);
 
+/* ---- distances to float sites and their gradient (no reference counterpart) -------------
+   dim = 2 (grid w x h, d = 1, sites as n x 2 floats) or 3 (w x h x d, n x 3
+   floats), in continuous cell coordinates (cell x covers [x, x+1)).
+   dol_sites_seed: the cell holding each site gets its mask bit; cell_site
+   (one int per cell) receives the smallest site index in the cell, a value
+   >= n_sites elsewhere.  Run a delta method (cw = 1) on the mask, then
+   dol_sites_forward: owner[p] = the site the cell's delta reaches (-1 if
+   none), dist[p] = |p - site| in fp32 with p the cell centre (NaN if none).
+   dol_sites_backward: with that owner assignment fixed,
+   grad_sites[k] = sum over cells p owned by k of grad_dist[p] *
+   (site_k - p) / |site_k - p| (segmented reduce by owner, fp64 accumulation,
+   fp32 result). */
+DOL_API dol_status dol_sites_seed(int dim, int w, int h, int d, int n_sites, const float* sites, uint32_t* mask,
+                                  int* cell_site, void* stream);
+DOL_API dol_status dol_sites_forward(int dim, int w, int h, int d, int n_sites, const void* deltas,
+                                     const int* cell_site, const float* sites, int* owner, float* dist, void* stream);
+DOL_API size_t     dol_sites_backward_workspace_size(int dim, int n_sites);
+DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites, const int* owner, const float* sites,
+                                      const float* grad_dist, float* grad_sites, void* workspace,
+                                      size_t workspace_bytes, void* stream);
+
 /* ---- synthetic inputs (no reference counterpart) --------------------------------------
    Integer-exact, so host and device give the same bits.  Value noise: lattice
    spacing `spacing`, lattice values in [0,65536) from the reference's LCG drawn

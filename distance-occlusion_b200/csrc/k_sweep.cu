@@ -44,6 +44,12 @@ __device__ __forceinline__ C3 cell_load_cg(const int16_t* p, long long i)
 }
 
 // ------------------------------------------------------------ Danielsson 2D ----
+// Rows 1..h-1 going down, then h-2..0 going up (:709-777): one "step" per row,
+// the row taking the previous step's row with a y offset of -cw (down) or
+// +cw (up), then an x pass to the right and one to the left.  The next step's
+// row is loaded during the current one, and each pass posts what the next
+// pass needs (row_pass), so a step costs two barriers when the passes settle
+// in one round.
 
 // One CTA runs the whole 2D Danielsson of one image (used by the single-image
 // kernel and by the batched kernel).
@@ -52,36 +58,45 @@ __device__ __forceinline__ void danielsson2_cta(uint32_t* __restrict__ dl, int w
 {
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
-    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const bool active = t < nseg;
+    const int n = active ? min(S, w - t * S) : 0;
     const long long x0 = (long long)t * S;
-    C2 P[S], C[S], Cn[S], V[S], R[S], D[S];
+    if (h < 2) return;
+    const int steps = 2 * (h - 1);
+    auto row_of = [&](int i) { return i < h - 1 ? i + 1 : 2 * h - 3 - i; };
+    auto dy_of = [&](int i) { return i < h - 1 ? -cw : cw; };
+    C2 P[S], C[S], V[S], R[S], D[S];
 #pragma unroll
-    for (int s = 0; s < S; s++) P[s] = C[s] = Cn[s] = V[s] = R[s] = D[s] = C2{0, 0};
+    for (int s = 0; s < S; s++) P[s] = C[s] = V[s] = R[s] = D[s] = C2{0, 0};
 
-    // down sweep, rows 1..h-1 (:709-741)
     load_row<C2, S>(P, dl, x0, n);
-    if (h > 1) load_row<C2, S>(C, dl, (long long)w + x0, n);
-    for (int y = 1; y < h; y++) {
-        if (y + 1 < h) load_row<C2, S>(Cn, dl, (long long)(y + 1) * w + x0, n);
+    load_row<C2, S>(C, dl, (long long)row_of(0) * w + x0, n);
 #pragma unroll
-        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, -cw));
-        row_pass<C2, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
-        row_pass<C2, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
+    for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, dy_of(0)));
+    int g = 0;
+    if (active) sh.guess[g][t] = seg_edge<C2, S, +1>(V, n);
+    __syncthreads();
+    for (int i = 0; i < steps; i++) {
+        const int y = row_of(i);
+        const bool more = i + 1 < steps;
+        const int dyn = more ? dy_of(i + 1) : 0;
+        if (more) load_row<C2, S>(C, dl, (long long)row_of(i + 1) * w + x0, n);
+        const C2 in0 = (active && t > 0) ? sh.guess[g][t - 1] : V[0];
+        row_pass<C2, S, false, +1>(R, V, t, nseg, n, cw, sh, D, in0, [&](const C2 (&X)[S]) {
+            if (active) sh.guess[g ^ 1][t] = X[0];
+        });
+        g ^= 1;
+        const C2 in1 = (active && t + 1 < nseg) ? sh.guess[g][t + 1] : R[0];
+        row_pass<C2, S, false, -1>(P, R, t, nseg, n, cw, sh, D, in1, [&](const C2 (&X)[S]) {
+            if (more && active)
+                sh.guess[g ^ 1][t] = closer(seg_edge<C2, S, +1>(C, n), add(seg_edge<C2, S, +1>(X, n), 0, dyn));
+        });
+        g ^= 1;
         store_row<C2, S>(dl, (long long)y * w + x0, P, n);
+        if (more) {
 #pragma unroll
-        for (int s = 0; s < S; s++) C[s] = Cn[s];
-    }
-    // up sweep, rows h-2..0 (:745-777); P holds row h-1
-    if (h > 1) load_row<C2, S>(C, dl, (long long)(h - 2) * w + x0, n);
-    for (int y = h - 2; y >= 0; y--) {
-        if (y >= 1) load_row<C2, S>(Cn, dl, (long long)(y - 1) * w + x0, n);
-#pragma unroll
-        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, +cw));
-        row_pass<C2, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
-        row_pass<C2, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
-        store_row<C2, S>(dl, (long long)y * w + x0, P, n);
-#pragma unroll
-        for (int s = 0; s < S; s++) C[s] = Cn[s];
+            for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, dyn));
+        }
     }
 }
 
@@ -94,8 +109,9 @@ __global__ void __launch_bounds__(512) k_danielsson2(uint32_t* __restrict__ dl, 
 
 // ------------------------------------------------------------ Danielsson 3D ----
 // Slices 1..d-1 then d-2..0 (:2355-2393); each slice takes the neighbouring
-// slice's cell with the z offset, then runs the 2D sweeps over its rows
-// (:2264-2345).  The z pull is folded into the first load of each row.
+// slice's cell with the z offset, then runs the 2D steps over its rows
+// (:2264-2345).  The z pull is folded into the first load of each row (rows of
+// the down sweep); the up sweep reads the down sweep's results.
 
 template <int S>
 __device__ __forceinline__ void danielsson3_cta(int16_t* __restrict__ dl, int w, int h, int d, int cw,
@@ -103,9 +119,13 @@ __device__ __forceinline__ void danielsson3_cta(int16_t* __restrict__ dl, int w,
 {
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
-    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const bool active = t < nseg;
+    const int n = active ? min(S, w - t * S) : 0;
     const long long x0 = (long long)t * S;
     const long long plane = (long long)w * h;
+    const int steps = 2 * (h - 1);
+    auto row_of = [&](int i) { return i < h - 1 ? i + 1 : 2 * h - 3 - i; };
+    auto dy_of = [&](int i) { return i < h - 1 ? -cw : cw; };
     C3 P[S], C[S], Q[S], V[S], R[S], D[S];
 #pragma unroll
     for (int s = 0; s < S; s++) P[s] = C[s] = Q[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
@@ -122,26 +142,48 @@ __device__ __forceinline__ void danielsson3_cta(int16_t* __restrict__ dl, int w,
 #pragma unroll
             for (int s = 0; s < S; s++) P[s] = closer(C[s], add(Q[s], 0, 0, dz));
             store_row<C3, S>(dl, sb + x0, P, n);
-            // down sweep
-            for (int y = 1; y < h; y++) {
-                const long long rb = sb + (long long)y * w + x0;
-                load_row<C3, S>(C, dl, rb, n);
-                load_row<C3, S>(Q, dl, pb + (long long)y * w + x0, n);
+            if (h < 2) continue;
+            // first step: row 1 of the down sweep (z pull, then y pull)
+            load_row<C3, S>(C, dl, sb + (long long)w + x0, n);
+            load_row<C3, S>(Q, dl, pb + (long long)w + x0, n);
 #pragma unroll
-                for (int s = 0; s < S; s++) V[s] = closer(closer(C[s], add(Q[s], 0, 0, dz)), add(P[s], 0, -cw, 0));
-                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
-                row_pass<C3, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
-                store_row<C3, S>(dl, rb, P, n);
-            }
-            // up sweep
-            for (int y = h - 2; y >= 0; y--) {
-                const long long rb = sb + (long long)y * w + x0;
-                load_row<C3, S>(C, dl, rb, n);
+            for (int s = 0; s < S; s++) V[s] = closer(closer(C[s], add(Q[s], 0, 0, dz)), add(P[s], 0, -cw, 0));
+            int g = 0;
+            __syncthreads();   // the previous slice's last pass may still read the guess slots
+            if (active) sh.guess[g][t] = seg_edge<C3, S, +1>(V, n);
+            __syncthreads();
+            for (int i = 0; i < steps; i++) {
+                const int y = row_of(i);
+                const bool more = i + 1 < steps;
+                const bool next_down = more && i + 1 < h - 1;
+                const int dyn = more ? dy_of(i + 1) : 0;
+                if (more) {
+                    const long long off = (long long)row_of(i + 1) * w + x0;
+                    load_row<C3, S>(C, dl, sb + off, n);
+                    if (next_down) load_row<C3, S>(Q, dl, pb + off, n);
+                }
+                const C3 in0 = (active && t > 0) ? sh.guess[g][t - 1] : V[0];
+                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, in0, [&](const C3 (&X)[S]) {
+                    if (active) sh.guess[g ^ 1][t] = X[0];
+                });
+                g ^= 1;
+                const C3 in1 = (active && t + 1 < nseg) ? sh.guess[g][t + 1] : R[0];
+                row_pass<C3, S, false, -1>(P, R, t, nseg, n, cw, sh, D, in1, [&](const C3 (&X)[S]) {
+                    if (more && active) {
+                        C3 c = seg_edge<C3, S, +1>(C, n);
+                        if (next_down) c = closer(c, add(seg_edge<C3, S, +1>(Q, n), 0, 0, dz));
+                        sh.guess[g ^ 1][t] = closer(c, add(seg_edge<C3, S, +1>(X, n), 0, dyn, 0));
+                    }
+                });
+                g ^= 1;
+                store_row<C3, S>(dl, sb + (long long)y * w + x0, P, n);
+                if (more) {
 #pragma unroll
-                for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, +cw, 0));
-                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
-                row_pass<C3, S, false, -1>(P, R, t, nseg, n, cw, sh, D, false);
-                store_row<C3, S>(dl, rb, P, n);
+                    for (int s = 0; s < S; s++) {
+                        C3 c = next_down ? closer(C[s], add(Q[s], 0, 0, dz)) : C[s];
+                        V[s] = closer(c, add(P[s], 0, dyn, 0));
+                    }
+                }
             }
         }
     }
@@ -158,53 +200,83 @@ __global__ void __launch_bounds__(512) k_danielsson3(int16_t* __restrict__ dl, i
 // Four quadrant sweeps; the first row of each sweep is left as is; each later
 // row takes the previous row's cell, then along x the previous cell of the row
 // and the diagonal cell of the previous row, in that order (:655-693).  The
-// previous row is also kept in shared memory for the diagonal candidates that
-// cross a segment boundary.
+// diagonal candidate of a segment's first cell is its predecessor's boundary
+// cell of the previous row, posted during the previous row's pass.
 
 template <int S>
 __global__ void __launch_bounds__(512) k_fastsweep2(uint32_t* __restrict__ dl, int w, int h, int cw)
 {
     __shared__ ScanShared<C2> sh;
-    extern __shared__ uint32_t prow[];   // [2][w]
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
-    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const bool active = t < nseg;
+    const int n = active ? min(S, w - t * S) : 0;
     const long long x0 = (long long)t * S;
     C2 P[S], C[S], V[S], R[S], D[S];
 #pragma unroll
     for (int s = 0; s < S; s++) P[s] = C[s] = V[s] = R[s] = D[s] = C2{0, 0};
+    if (h < 2) return;
 
     for (int sweep = 0; sweep < 4; sweep++) {
         const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1;
         const int ox = -cw * dx, oy = -cw * dy;
         const int y0 = dy > 0 ? 0 : h - 1;
-        int buf = 0;
+        const int pred = t - dx;   // predecessor in this sweep's scan order
+        const bool has_pred = active && pred >= 0 && pred < nseg;
         load_row<C2, S>(P, dl, (long long)y0 * w + x0, n);
+        load_row<C2, S>(C, dl, (long long)(y0 + dy) * w + x0, n);
 #pragma unroll
-        for (int s = 0; s < S; s++)
-            if (s < n) prow[buf * w + x0 + s] = pack2(P[s]);
+        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, oy));
+        int g = 0;
+        __syncthreads();   // the previous sweep's last pass may still read the slots
+        if (active) {
+            sh.guess[g][t] = dx > 0 ? seg_edge<C2, S, +1>(V, n) : seg_edge<C2, S, -1>(V, n);
+            sh.edge[g][t] = dx > 0 ? seg_edge<C2, S, +1>(P, n) : seg_edge<C2, S, -1>(P, n);
+        }
         __syncthreads();
         for (int j = 1; j < h; j++) {
             const int y = y0 + j * dy;
-            load_row<C2, S>(C, dl, (long long)y * w + x0, n);
+            const bool more = j + 1 < h;
+            if (more) load_row<C2, S>(C, dl, (long long)(y + dy) * w + x0, n);
+            // diagonal candidates from the previous row (P): own cells, then the predecessor's edge
+            if (dx > 0) {
 #pragma unroll
-            for (int s = 0; s < S; s++) {
-                V[s] = closer(C[s], add(P[s], 0, oy));
-                const long long xp = x0 + s - dx;
-                if (s < n && xp >= 0 && xp < w) D[s] = add(unpack2(prow[buf * w + xp]), ox, oy);
+                for (int s = 1; s < S; s++) D[s] = add(P[s - 1], ox, oy);
+            } else {
+#pragma unroll
+                for (int s = 0; s + 1 < S; s++) D[s] = add(P[s + 1], ox, oy);
             }
+            if (has_pred) {
+                const C2 e = add(sh.edge[g][pred], ox, oy);
+                if (dx > 0) D[0] = e;
+                else {
+#pragma unroll
+                    for (int s = 0; s < S; s++)
+                        if (s == n - 1) D[s] = e;
+                }
+            }
+            const C2 in0 = has_pred ? sh.guess[g][pred] : V[0];
+            auto post = [&](const C2 (&X)[S]) {
+                if (!active) return;
+                if (dx > 0) {
+                    sh.edge[g ^ 1][t] = seg_edge<C2, S, +1>(X, n);
+                    if (more) sh.guess[g ^ 1][t] = closer(seg_edge<C2, S, +1>(C, n), add(seg_edge<C2, S, +1>(X, n), 0, oy));
+                } else {
+                    sh.edge[g ^ 1][t] = seg_edge<C2, S, -1>(X, n);
+                    if (more) sh.guess[g ^ 1][t] = closer(seg_edge<C2, S, -1>(C, n), add(seg_edge<C2, S, -1>(X, n), 0, oy));
+                }
+            };
             if (dx > 0)
-                row_pass<C2, S, true, +1>(R, V, t, nseg, n, cw, sh, D, false);
+                row_pass<C2, S, true, +1>(R, V, t, nseg, n, cw, sh, D, in0, post);
             else
-                row_pass<C2, S, true, -1>(R, V, t, nseg, n, cw, sh, D, false);
+                row_pass<C2, S, true, -1>(R, V, t, nseg, n, cw, sh, D, in0, post);
+            g ^= 1;
             store_row<C2, S>(dl, (long long)y * w + x0, R, n);
-            buf ^= 1;
 #pragma unroll
             for (int s = 0; s < S; s++) {
                 P[s] = R[s];
-                if (s < n) prow[buf * w + x0 + s] = pack2(R[s]);
+                if (more) V[s] = closer(C[s], add(P[s], 0, oy));
             }
-            __syncthreads();
         }
     }
 }
@@ -221,7 +293,8 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
     __shared__ int s_item;
     const int t = threadIdx.x;
     const int nseg = (w + S - 1) / S;
-    const int n = t < nseg ? min(S, w - t * S) : 0;
+    const bool active = t < nseg;
+    const int n = active ? min(S, w - t * S) : 0;
     const long long x0 = (long long)t * S;
     const long long plane = (long long)w * h;
     const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1, dz = (sweep & 4) ? -1 : 1;
@@ -229,6 +302,8 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
     const int yb = dy > 0 ? 0 : h - 1, zb = dz > 0 ? 0 : d - 1;
     const int H = h - 1, Dd = d - 1;
     const long long total = (long long)H * Dd;
+    const int pred = t - dx;
+    const bool has_pred = active && pred >= 0 && pred < nseg;
     C3 C[S], Zp[S], Yp[S], V[S], R[S], D[S];
 #pragma unroll
     for (int s = 0; s < S; s++) C[s] = Zp[s] = Yp[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
@@ -276,10 +351,14 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
                 Yp[s] = cell_load_cg(dl, yb_ + s);
                 V[s] = closer(closer(C[s], add(Zp[s], 0, 0, oz)), add(Yp[s], 0, oy, 0));
             }
+        if (active) sh.guess[0][t] = dx > 0 ? seg_edge<C3, S, +1>(V, n) : seg_edge<C3, S, -1>(V, n);
+        __syncthreads();
+        const C3 in0 = has_pred ? sh.guess[0][pred] : V[0];
+        auto nopost = [](const C3 (&)[S]) {};
         if (dx > 0)
-            row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, false);
+            row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, in0, nopost);
         else
-            row_pass<C3, S, false, -1>(R, V, t, nseg, n, cw, sh, D, false);
+            row_pass<C3, S, false, -1>(R, V, t, nseg, n, cw, sh, D, in0, nopost);
         store_row<C3, S>(dl, rb, R, n);
         __threadfence();
         __syncthreads();
@@ -333,14 +412,11 @@ void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st)
 {
     const int s = pick_s(w, 512);
     const int T = threads_for(w, s);
-    const size_t smem = 2 * (size_t)w * sizeof(uint32_t);
     ProfScope ps("fastsweep_2d", st);
 #define DOL_FS_CASE(SV)                                                                                      \
-    case SV: {                                                                                               \
-        auto kern = k_fastsweep2<SV>;                                                                        \
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                 \
-        kern<<<1, T, smem, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);                                  \
-    } break;
+    case SV:                                                                                                 \
+        k_fastsweep2<SV><<<1, T, 0, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);                         \
+        break;
     switch (s) {
         DOL_FS_CASE(1)
         DOL_FS_CASE(2)

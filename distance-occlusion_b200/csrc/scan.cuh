@@ -10,36 +10,42 @@
 // change along the row, so this is not an associative scan: the result depends
 // on the exact chain of replacements.  It is still a composition of per-cell
 // functions v -> f_i(v), so a row split into segments (S cells per thread) can
-// be solved by iterating to the unique fixed point:
+// be solved by iterating segment inputs to the unique fixed point:
 //
-//   round 0   each segment guesses its input (the neighbour's value before the
-//             pass) and runs its cells serially;
-//   round r   each segment takes as input the output of the nearest segment
-//             before it that did NOT simply pass its input through (a segment
-//             whose output equals its input shifted by its length is
-//             "transparent"), shifted across the transparent segments between;
+//   round 0   each segment takes as input its predecessor's boundary cell as
+//             it was before the pass (published during the previous pass);
+//   round r   each segment takes the output of the nearest segment before it
+//             that did NOT pass its input through unchanged ("transparent":
+//             output == input shifted by the segment length), shifted across
+//             the transparent segments in between;
 //   stop      when every segment's input equals its predecessor's output.
 //
-// At the stop every segment's input is exactly what the serial pass would feed
-// it, so the result is bit-identical to the serial pass.  Termination: if
-// segments 0..k are correct after round r, segment k+1 is correct after round
-// r+1 (its jump source is correct and everything between passed the correct
-// value through), so at most (segments) rounds; on real rows it is 1-3 rounds,
-// and the transparent-jump rule is what keeps long chains (a seed's influence
-// crossing an empty row) to a few rounds instead of one round per segment.
+// At the stop every input is what the serial pass would feed that segment, so
+// the result is bit-identical to the serial pass.  It terminates: if segments
+// 0..k are right after round r, segment k+1 is right after round r+1 (its
+// jump source is right and everything between passed the right value on), so
+// at most one round per segment; measured rows take 1-3 rounds, the jump rule
+// keeping long chains (a seed's influence crossing an empty row) short.
+//
+// One barrier per round: a thread can tell by itself whether its successor's
+// input was right, because that input is either the thread's own output (the
+// thread was not transparent) or its own input shifted by its length (it
+// was); so each thread checks its successor and a single __syncthreads_or
+// both publishes the round's outputs and decides whether another round runs.
 #pragma once
 
 #include "common.cuh"
 
 namespace dolk {
 
+constexpr int kMaxScanThreads = 512;
+
 template <class Cell>
 struct ScanShared {
-    // per round parity: each thread's segment output, and per warp a ballot of
-    // the threads whose segment was not transparent
-    Cell out[2][1024];
-    uint32_t nt[2][32];
-    Cell guess[1024];
+    Cell out[2][kMaxScanThreads];     // segment outputs, by round parity
+    uint32_t nt[2][32];               // per warp: ballot of non-transparent segments, by round parity
+    Cell guess[2][kMaxScanThreads];   // boundary cells published for the next pass, by pass parity
+    Cell edge[2][kMaxScanThreads];    // FastSweep 2D: each segment's boundary cell of the previous row
 };
 
 // Load/store helpers for row cells.  2D cells are one uint32; 3D cells three int16.
@@ -58,6 +64,21 @@ DOL_HD void cell_store(int16_t* p, long long i, C3 c)
     o[2] = (int16_t)c.z;
 }
 
+// The boundary cell of a segment on the side its successor sees in scan
+// direction dir: the last live cell for dir > 0, the first for dir < 0.
+// (Unrolled select, so the register array is never indexed dynamically.)
+template <class Cell, int S, int dir>
+__device__ __forceinline__ Cell seg_edge(const Cell (&A)[S], int n)
+{
+    Cell e = A[0];
+    if (dir > 0) {
+#pragma unroll
+        for (int s = 1; s < S; s++)
+            if (s < n) e = A[s];
+    }
+    return e;
+}
+
 // Segment-local serial pass.  dir = +1: cells 0..n-1, chain shift -cw;
 // dir = -1: cells n-1..0, chain shift +cw (a template argument, so the
 // register arrays stay in registers).  D (FastSweep 2D) holds the
@@ -74,8 +95,6 @@ __device__ __forceinline__ Cell seg_pass(Cell (&R)[S], const Cell (&V)[S], int n
         const int s = dir > 0 ? u : S - 1 - u;
         if (s < n) {
             Cell v = V[s];
-            // both the chain and the diagonal candidate exist iff a cell precedes
-            // this one in the row's scan order
             if (have) {
                 v = closer(v, addx(cur, -dir * cw));
                 if (kDiag) v = closer(v, D[s]);
@@ -89,75 +108,68 @@ __device__ __forceinline__ Cell seg_pass(Cell (&R)[S], const Cell (&V)[S], int n
 }
 
 // The row pass over the whole CTA.  t: thread index; nseg: threads holding
-// cells; n: cells of this thread (0 if none).  Exact; see the file comment.
-template <class Cell, int S, bool kDiag, int dir>
+// cells; n: cells of this thread (0 if none); in0: this segment's round-0
+// input (its predecessor's boundary cell before the pass).  `publish(R)` runs
+// after every round, before the round's barrier: the caller uses it to post
+// what the NEXT pass needs from this thread, so the final round's post is
+// visible to all threads when this function returns.
+template <class Cell, int S, bool kDiag, int dir, class Pub>
 __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t, int nseg, int n, int cw,
-                                         ScanShared<Cell>& sh, const Cell (&D)[S], bool row_first_diag_ok)
+                                         ScanShared<Cell>& sh, const Cell (&D)[S], Cell in0, Pub&& publish)
 {
     const int lane = t & 31, wi = t >> 5;
     const bool active = t < nseg;
-    // scan-order index of this segment and of its predecessor's thread
-    const int sigma = dir > 0 ? t : nseg - 1 - t;
-    const int pred = t - dir;
+    const int sigma = dir > 0 ? t : nseg - 1 - t;   // position in scan order
     const bool has_pred = active && sigma > 0;
-    (void)row_first_diag_ok;
+    const bool has_succ = active && sigma < nseg - 1;
 
-    // round 0 guess: the predecessor's boundary cell before the pass
-    Cell edge = V[0];
-    if (dir > 0) {
-#pragma unroll
-        for (int s = 1; s < S; s++)
-            if (s < n) edge = V[s];
-    }
-    if (active) sh.guess[t] = edge;
-    __syncthreads();
-    Cell in = has_pred ? sh.guess[pred] : V[0];
-    bool has_in = has_pred;
-
+    Cell in = in0;
+    Cell succ_in = seg_edge<Cell, S, dir>(V, n);   // what my successor takes in round 0
     for (int r = 0;; r++) {
         const int b = r & 1;
-        Cell out = seg_pass<Cell, S, kDiag, dir>(R, V, n, cw, in, has_in, D);
-        const bool trans = has_in && same(out, addx(in, -dir * cw * n));
+        const Cell out = seg_pass<Cell, S, kDiag, dir>(R, V, n, cw, in, has_pred, D);
+        publish(R);
+        const bool trans = has_pred && same(out, addx(in, -dir * cw * n));
         if (active) sh.out[b][t] = out;
         const uint32_t nt = __ballot_sync(0xFFFFFFFFu, active && !trans);
         if (lane == 0) sh.nt[b][wi] = nt;
-        __syncthreads();
+        const bool bad = has_succ && !same(succ_in, out);
+        // the cap only keeps a logic error from looping on the device; the
+        // fixed point is reached within nseg rounds
+        if (!__syncthreads_or(bad) || r > nseg + 2) break;
 
-        bool bad = has_pred && !same(in, sh.out[b][pred]);
-        // next input: the nearest non-transparent segment before us in scan order
-        Cell nin = in;
+        // round r+1 input: nearest non-transparent segment before us in scan order
         if (has_pred) {
             int j = -1;
             if (dir > 0) {
-                uint32_t below = nt & ((1u << lane) - 1u);
+                const uint32_t below = nt & ((1u << lane) - 1u);
                 if (below) {
                     j = (wi << 5) + 31 - __clz(below);
                 } else {
                     for (int ww = wi - 1; ww >= 0; ww--) {
-                        uint32_t m = sh.nt[b][ww];
+                        const uint32_t m = sh.nt[b][ww];
                         if (m) { j = (ww << 5) + 31 - __clz(m); break; }
                     }
                 }
             } else {
-                uint32_t above = lane == 31 ? 0u : (nt & ~((2u << lane) - 1u));
+                const uint32_t above = lane == 31 ? 0u : (nt & ~((2u << lane) - 1u));
                 if (above) {
                     j = (wi << 5) + __ffs(above) - 1;
                 } else {
                     const int nwarps = (nseg + 31) >> 5;
                     for (int ww = wi + 1; ww < nwarps; ww++) {
-                        uint32_t m = sh.nt[b][ww];
+                        const uint32_t m = sh.nt[b][ww];
                         if (m) { j = (ww << 5) + __ffs(m) - 1; break; }
                     }
                 }
             }
             // j exists: the first segment in scan order is never transparent
             const int gap = (dir > 0 ? t - j : j - t) - 1;   // full segments in between
-            nin = addx(sh.out[b][j], -dir * cw * S * gap);
+            in = addx(sh.out[b][j], -dir * cw * S * gap);
         }
-        // the fixed point is reached within nseg rounds; the cap only guards
-        // against a logic error turning into an endless loop on the device
-        if (!__syncthreads_or(bad) || r > nseg + 2) break;
-        in = nin;
+        // my successor's round r+1 input, by the same rule: my output, or (if I
+        // passed my input through) my new input carried across my cells
+        succ_in = trans ? addx(in, -dir * cw * n) : out;
     }
 }
 

@@ -296,42 +296,37 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     const long long base = (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-    const int qstep = kRowsPerWarp * nw;
-
-    // Each lane walks its own queue of positions q, q + qstep, ...; one loop
-    // iteration is one probe step of the current position, and a lane that
-    // finishes a position starts its next one in the same iteration, so lanes
-    // with short searches do not wait for the warp's longest one.  Probes past
-    // the line's ends are clamped to the end cell: that cell was already
-    // probed at a smaller k, so a clamped probe can never lower the minimum.
-    int q = kRowsPerWarp * wi + sub;
-    uint32_t s = 0, best = 0, k2 = 0, dk = 0;
-    int k = 0, reach = 0;
-    const TIn* A = F0 + col;
-    bool fresh = true;
-    for (;;) {
-        if (fresh) {
-            if (q >= n) break;
-            s = F1[q * TX + col] != 0;   // every own value is >= 1
-            A = (s ? F1 : F0) + col;
-            best = sq_val<TIn>(A[q * TX]);
-            k = 1;
-            k2 = 1;
-            dk = 3;
-            reach = max(q, n - 1 - q);
-            fresh = false;
+    // The lanes of a warp take adjacent positions and step k together, so
+    // each probe of the warp reads (32/TX) adjacent tile rows: conflict-free.
+    for (int q = kRowsPerWarp * wi + sub; q < n; q += kRowsPerWarp * nw) {
+        const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
+        const TIn* A = (s ? F1 : F0) + col;
+        uint32_t best = sq_val<TIn>(A[q * TX]);
+        const int lmax = q, rmax = n - 1 - q, kmin = min(lmax, rmax);
+        uint32_t k2 = 1, dk = 3;
+        int k = 1;
+        const TIn* pl = A + (q - 1) * TX;
+        const TIn* pr = A + (q + 1) * TX;
+        for (; k <= kmin && k2 < best; k++) {
+            best = min(best, min(sq_val<TIn>(*pl), sq_val<TIn>(*pr)) + k2);
+            pl -= TX;
+            pr += TX;
+            k2 += dk;
+            dk += 2;
         }
-        if (k2 >= best || k > reach) {
-            put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
-            q += qstep;
-            fresh = true;
-            continue;
+        for (; k <= lmax && k2 < best; k++) {
+            best = min(best, sq_val<TIn>(*pl) + k2);
+            pl -= TX;
+            k2 += dk;
+            dk += 2;
         }
-        const int il = max(q - k, 0), ir = min(q + k, n - 1);
-        best = min(best, min(sq_val<TIn>(A[il * TX]), sq_val<TIn>(A[ir * TX])) + k2);
-        k++;
-        k2 += dk;
-        dk += 2;
+        for (; k <= rmax && k2 < best; k++) {
+            best = min(best, sq_val<TIn>(*pr) + k2);
+            pr += TX;
+            k2 += dk;
+            dk += 2;
+        }
+        put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }
 }
 

@@ -415,7 +415,9 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
             auto kern = k_edt_line_tma<TIn, kFinal, TX>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
-            kern<<<grid, 512, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err);
+            const int tv = tune_get(kTuneEdt, w);
+            const int threads = tv == 256 ? 256 : 512;
+            kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err);
             return;
         }
     }

@@ -11,11 +11,11 @@
 
 namespace dolk {
 
-__global__ void __launch_bounds__(256) k_jfa2(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int w,
+__global__ void __launch_bounds__(512) k_jfa2(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int w,
                                               int h, int s, int cw)
 {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int y = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (x >= w || y >= h) return;
     const int o = cw * s;
     auto at = [&](int xx, int yy) { return unpack2(__ldg(in + (long long)yy * w + xx)); };
@@ -49,11 +49,11 @@ __device__ __forceinline__ void store3(int16_t* p, long long i, C3 v)
     c[2] = (int16_t)v.z;
 }
 
-__global__ void __launch_bounds__(256) k_jfa3(const int16_t* __restrict__ in, int16_t* __restrict__ out, int w, int h,
+__global__ void __launch_bounds__(512) k_jfa3(const int16_t* __restrict__ in, int16_t* __restrict__ out, int w, int h,
                                               int d, int s, int cw)
 {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int y = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int z = blockIdx.z;
     if (x >= w || y >= h) return;
     const long long plane = (long long)w * h;
@@ -90,14 +90,19 @@ void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, in
     if (dim == 3 && d > m) m = d;
     void* a = deltas;
     void* b = temp;
+    // rows per CTA (32 x ry threads): tuned, else 8
+    int ry = tune_get(dim == 2 ? kTuneJfa2 : kTuneJfa3, w);
+    if (ry != 2 && ry != 4 && ry != 8 && ry != 16) ry = 8;
     auto pass = [&](int s, const void* src, void* dst) {
         ProfScope ps("jumpflood_pass", st);
         if (dim == 2) {
-            dim3 grid((w + 31) / 32, (h + 7) / 8);
-            k_jfa2<<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), w, h, s, cw);
+            dim3 grid((w + 31) / 32, (h + ry - 1) / ry);
+            k_jfa2<<<grid, 32 * ry, 0, st>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), w, h, s,
+                                             cw);
         } else {
-            dim3 grid((w + 31) / 32, (h + 7) / 8, d);
-            k_jfa3<<<grid, 256, 0, st>>>(static_cast<const int16_t*>(src), static_cast<int16_t*>(dst), w, h, d, s, cw);
+            dim3 grid((w + 31) / 32, (h + ry - 1) / ry, d);
+            k_jfa3<<<grid, 32 * ry, 0, st>>>(static_cast<const int16_t*>(src), static_cast<int16_t*>(dst), w, h, d, s,
+                                             cw);
         }
     };
     for (int s = floor_pow2(m - 1); s > 0; s /= 2) {

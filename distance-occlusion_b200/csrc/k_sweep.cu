@@ -380,6 +380,14 @@ static int pick_s(int w, int max_threads)
     return 0;
 }
 
+// the tuned cells-per-thread for this family and width, if it fits
+static int tuned_s(int kind, int w, int max_threads)
+{
+    const int v = tune_get(kind, w);
+    if ((v == 1 || v == 2 || v == 4 || v == 8) && (w + v - 1) / v <= max_threads) return v;
+    return pick_s(w, max_threads);
+}
+
 static int threads_for(int w, int s)
 {
     int n = (w + s - 1) / s;
@@ -388,7 +396,7 @@ static int threads_for(int w, int s)
 
 void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st)
 {
-    const int s = pick_s(w, 512);
+    const int s = tuned_s(dim == 2 ? kTuneDan2 : kTuneDan3, w, 512);
     const int T = threads_for(w, s);
     ProfScope ps("danielsson", st);
 #define DOL_DAN_CASE(SV)                                                                              \
@@ -410,7 +418,7 @@ void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaS
 
 void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st)
 {
-    const int s = pick_s(w, 512);
+    const int s = tuned_s(kTuneFs2, w, 512);
     const int T = threads_for(w, s);
     ProfScope ps("fastsweep_2d", st);
 #define DOL_FS_CASE(SV)                                                                                      \
@@ -467,7 +475,7 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
     cudaMemsetAsync(flags, 0, (size_t)h * d * sizeof(int), st);
     cudaMemsetAsync(counters, 0, 8 * sizeof(int), st);
 
-    const int s = pick_s(w, 256);
+    const int s = tuned_s(kTuneFs3, w, 256);
     const int T = threads_for(w, s);
     ProfScope ps("fastsweep_3d", st);
 #define DOL_FS3_CASE(SV)                                                                                     \
@@ -592,15 +600,25 @@ void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t
                       int* counter, cudaStream_t st)
 {
     ProfScope ps("batch_sdf", st);
+    // rows up to 1024 cells: 4 cells x 256 threads, or 8 cells x 128 threads
+    const bool eight = tune_get(kTuneBatch, 1024) == 8;
+    const int threads = eight ? 128 : 256;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_sdf<4>, 256, 0);
+    if (eight)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_sdf<8>, threads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_sdf<4>, threads, 0);
     if (per_sm < 1) per_sm = 1;
     int grid = per_sm * g_num_sms;
     if (grid > n) grid = n;
     if (grid < 1) grid = 1;
     cudaMemsetAsync(counter, 0, sizeof(int), st);
-    k_batch_sdf<4><<<grid, 256, 0, st>>>(static_cast<const BatchItemDev*>(items), order, n, masks,
-                                         static_cast<unsigned char*>(deltas), dist, counter);
+    if (eight)
+        k_batch_sdf<8><<<grid, threads, 0, st>>>(static_cast<const BatchItemDev*>(items), order, n, masks,
+                                                 static_cast<unsigned char*>(deltas), dist, counter);
+    else
+        k_batch_sdf<4><<<grid, threads, 0, st>>>(static_cast<const BatchItemDev*>(items), order, n, masks,
+                                                 static_cast<unsigned char*>(deltas), dist, counter);
 }
 
 }  // namespace dolk

@@ -24,6 +24,12 @@ private:
 // records the message returned by dol_last_error() and returns `s`
 int set_error(int s, const char* fmt, ...);
 
+// launch-configuration table (tune.cu); values are family specific, 0 = use
+// the launcher's heuristic.  The order matches the DOL_TUNE_* constants.
+enum TuneKind { kTuneDan2 = 0, kTuneDan3, kTuneFs2, kTuneFs3, kTuneJfa2, kTuneJfa3, kTuneBatch, kTuneEdt, kTuneKinds };
+int tune_get(int kind, int w);
+void tune_put(int kind, int w, int value);
+
 inline uint32_t float_bits(float f)
 {
     uint32_t u;

@@ -235,6 +235,25 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
                                       const float* grad_dist, float* grad_sites, void* workspace,
                                       size_t workspace_bytes, void* stream);
 
+/* ---- autotuning (no reference counterpart) ---------------------------------------------
+   Launch parameters that change speed but never results: cells per thread of
+   the row sweeps, rows per CTA of the JumpFlood passes, threads per CTA of the
+   EDT line passes, the CTA shape of the batched kernel.  They are kept per
+   device and per size bucket (ceil(log2(w))); 0 = the built-in heuristic.
+   dol_autotune times every candidate on a synthetic problem of the given shape
+   (blocking; it allocates its own scratch) and keeps the fastest. */
+#define DOL_TUNE_DANIELSSON_2D 0   /* cells per thread: 1, 2, 4, 8 */
+#define DOL_TUNE_DANIELSSON_3D 1
+#define DOL_TUNE_FASTSWEEP_2D  2
+#define DOL_TUNE_FASTSWEEP_3D  3
+#define DOL_TUNE_JUMPFLOOD_2D  4   /* rows per CTA: 2, 4, 8, 16 */
+#define DOL_TUNE_JUMPFLOOD_3D  5
+#define DOL_TUNE_BATCH         6   /* cells per thread: 4 (256 threads) or 8 (128 threads) */
+#define DOL_TUNE_EDT           7   /* threads per CTA of the line passes: 256 or 512 */
+DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream);
+DOL_API int        dol_tune_get(int kind, int w);
+DOL_API void       dol_tune_set(int kind, int w, int value);
+
 /* ---- synthetic inputs (no reference counterpart) --------------------------------------
    Integer-exact, so host and device give the same bits.  Value noise: lattice
    spacing `spacing`, lattice values in [0,65536) from the reference's LCG drawn

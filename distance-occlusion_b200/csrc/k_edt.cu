@@ -238,17 +238,10 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
 // TMA form.  A TX-column x full-line tile arrives in 256-position boxes
 // (cp.async.bulk.tensor, one mbarrier).  It is then split in place into two
 // state-specific arrays: F_s[p] is the cell's value (v or e) when its state is
-// s and 0 otherwise, so a cell of state s minimises (q - p)^2 + F_s[p] over p.
-//
-// The leftmost minimiser a(q) of that line problem never decreases with q
-// (the cost (q - p)^2 + F(p) is a Monge array), so the positions are solved in
-// four levels: every 8th position (and the last) by a full outward search,
-// then the positions 4 mod 8, 2 mod 4 and the odd ones by scanning only
-// [a(q - h), a(q + h)] between their already-solved neighbours at distance h.
-// Neighbours of the other state need no lookup: under F_s their minimiser is
-// themselves (their own value is 0).  Measured on the value-noise volume this
-// probes ~2.2x fewer cells than searching every position, and the short
-// bounded scans diverge less.
+// s and 0 otherwise, so for a cell of state s every probe is one load, one
+// multiply-add (or add) and one min -- a cell of the other state at distance k
+// contributes exactly k^2.  The symmetric part of the walk runs without bounds
+// checks; lanes cover TX columns x (32/TX) adjacent positions.
 template <typename TIn>
 __device__ __forceinline__ uint32_t sq_val(TIn v)
 {
@@ -263,9 +256,8 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
     const int rows = nbox * 256;
-    TIn* F0 = reinterpret_cast<TIn*>(smem_raw);          // [rows][TX], first the raw tile
-    TIn* F1 = F0 + rows * TX;                             // [rows][TX]
-    uint16_t* AR = reinterpret_cast<uint16_t*>(F1 + rows * TX);   // [n][TX] leftmost minimisers
+    TIn* F0 = reinterpret_cast<TIn*>(smem_raw);   // [rows][TX], first the raw tile
+    TIn* F1 = F0 + rows * TX;                      // [rows][TX]
     __shared__ __align__(8) uint64_t bar;
     const int x0 = blockIdx.x * TX;
     const int outer = blockIdx.y;
@@ -298,79 +290,43 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     }
     __syncthreads();
 
+    constexpr int kRowsPerWarp = 32 / TX;
+    const int lane = threadIdx.x & 31, col = lane % TX, sub = lane / TX;
+    const int nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
+    const int x = x0 + col;
+    if (x >= w) return;
+    const long long base = (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-    const int cols = min(TX, w - x0);
-    const long long obase = (long long)outer * outer_stride + x0;
-    auto state_at = [&](int q, int c) -> uint32_t { return F1[q * TX + c] != 0; };   // own values are >= 1
-    auto emit = [&](int q, int c, uint32_t s, uint32_t best) {
-        put_line_value<kFinal>(out, obase + c + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
-    };
-
-    // level 0: positions 0, 8, 16, ... and n-1, full search for the leftmost minimiser
-    const int n0 = (n + 7) >> 3;
-    const bool extra = ((n - 1) & 7) != 0;   // n-1 is not already a multiple of 8
-    for (int i = threadIdx.x; i < (n0 + (extra ? 1 : 0)) * TX; i += blockDim.x) {
-        const int c = i % TX, j = i / TX;
-        if (c >= cols) continue;
-        const int q = j < n0 ? 8 * j : n - 1;
-        const uint32_t s = state_at(q, c);
-        const TIn* A = (s ? F1 : F0) + c;
+    for (int q = kRowsPerWarp * wi + sub; q < n; q += kRowsPerWarp * nw) {
+        const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
+        const TIn* A = (s ? F1 : F0) + col;
         uint32_t best = sq_val<TIn>(A[q * TX]);
-        int arg = q;
         const int lmax = q, rmax = n - 1 - q, kmin = min(lmax, rmax);
         uint32_t k2 = 1, dk = 3;
         int k = 1;
-        // a left candidate that ties the best has the smallest index so far: take it;
-        // a right candidate only when strictly better (k^2 == best may still tie on the left)
-        for (; k <= kmin && k2 <= best; k++) {
-            const uint32_t cl = sq_val<TIn>(A[(q - k) * TX]) + k2;
-            if (cl <= best) { best = cl; arg = q - k; }
-            const uint32_t cr = sq_val<TIn>(A[(q + k) * TX]) + k2;
-            if (cr < best) { best = cr; arg = q + k; }
+        const TIn* pl = A + (q - 1) * TX;
+        const TIn* pr = A + (q + 1) * TX;
+        for (; k <= kmin && k2 < best; k++) {
+            best = min(best, min(sq_val<TIn>(*pl), sq_val<TIn>(*pr)) + k2);
+            pl -= TX;
+            pr += TX;
             k2 += dk;
             dk += 2;
         }
-        for (; k <= lmax && k2 <= best; k++) {
-            const uint32_t cl = sq_val<TIn>(A[(q - k) * TX]) + k2;
-            if (cl <= best) { best = cl; arg = q - k; }
+        for (; k <= lmax && k2 < best; k++) {
+            best = min(best, sq_val<TIn>(*pl) + k2);
+            pl -= TX;
             k2 += dk;
             dk += 2;
         }
         for (; k <= rmax && k2 < best; k++) {
-            const uint32_t cr = sq_val<TIn>(A[(q + k) * TX]) + k2;
-            if (cr < best) { best = cr; arg = q + k; }
+            best = min(best, sq_val<TIn>(*pr) + k2);
+            pr += TX;
             k2 += dk;
             dk += 2;
         }
-        AR[q * TX + c] = (uint16_t)arg;
-        emit(q, c, s, best);
-    }
-    __syncthreads();
-
-    // levels 1-3: offsets 4, 2, 1 between solved neighbours at distance h
-    for (int h = 4; h >= 1; h >>= 1) {
-        const int npos = (n - h + 2 * h - 1) / (2 * h);   // q = h, 3h, 5h, ... < n
-        for (int i = threadIdx.x; i < npos * TX; i += blockDim.x) {
-            const int c = i % TX, j = i / TX;
-            const int q = h + 2 * h * j;
-            if (c >= cols || q == n - 1) continue;   // n-1 was solved at level 0
-            const uint32_t s = state_at(q, c);
-            const TIn* A = (s ? F1 : F0) + c;
-            const int ql = q - h, qr = min(q + h, n - 1);
-            const int lo = state_at(ql, c) == s ? AR[ql * TX + c] : ql;
-            const int hi = state_at(qr, c) == s ? AR[qr * TX + c] : qr;
-            uint32_t best = 0xFFFFFFFFu;
-            int arg = lo;
-            for (int p = lo; p <= hi; p++) {
-                const int dq = q - p;
-                const uint32_t cv = sq_val<TIn>(A[p * TX]) + (uint32_t)(dq * dq);
-                if (cv < best) { best = cv; arg = p; }
-            }
-            AR[q * TX + c] = (uint16_t)arg;
-            emit(q, c, s, best);
-        }
-        __syncthreads();
+        put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }
 }
 
@@ -403,7 +359,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const long long outer_stride = along_z ? w : plane;
     constexpr int TX = sizeof(TIn) == 2 ? 16 : 8;   // 32-byte box rows either way
     const int nbox = (n + 255) / 256;
-    const size_t tile_bytes = 2 * (size_t)nbox * 256 * TX * sizeof(TIn) + (size_t)n * TX * sizeof(uint16_t);
+    const size_t tile_bytes = 2 * (size_t)nbox * 256 * TX * sizeof(TIn);
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
     CUtensorMap map;
     if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {

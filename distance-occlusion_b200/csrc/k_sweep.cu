@@ -366,6 +366,174 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
     }
 }
 
+// ------------------------------------------------------- single-warp engines ----
+// Rows of at most 32*S cells: one warp per image (or volume), every exchange a
+// shuffle, no shared memory and no CTA barrier (row_pass_warp).  Same steps
+// and candidate order as the CTA engines above.
+
+template <int S>
+__device__ __forceinline__ void danielsson2_warp(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    const int lane = threadIdx.x & 31;
+    const int nseg = (w + S - 1) / S;
+    const bool active = lane < nseg;
+    const int n = active ? min(S, w - lane * S) : 0;
+    const long long x0 = (long long)lane * S;
+    if (h < 2) return;
+    const int steps = 2 * (h - 1);
+    auto row_of = [&](int i) { return i < h - 1 ? i + 1 : 2 * h - 3 - i; };
+    auto dy_of = [&](int i) { return i < h - 1 ? -cw : cw; };
+    C2 P[S], C[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = V[s] = R[s] = D[s] = C2{0, 0};
+    load_row<C2, S>(P, dl, x0, n);
+    load_row<C2, S>(C, dl, (long long)row_of(0) * w + x0, n);
+#pragma unroll
+    for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, dy_of(0)));
+    for (int i = 0; i < steps; i++) {
+        const int y = row_of(i);
+        const bool more = i + 1 < steps;
+        if (more) load_row<C2, S>(C, dl, (long long)row_of(i + 1) * w + x0, n);
+        row_pass_warp<C2, S, false, +1>(R, V, lane, nseg, n, cw, D, warp_round0_input<C2, S, +1>(V, n, lane));
+        row_pass_warp<C2, S, false, -1>(P, R, lane, nseg, n, cw, D, warp_round0_input<C2, S, -1>(R, n, lane));
+        store_row<C2, S>(dl, (long long)y * w + x0, P, n);
+        if (more) {
+            const int dyn = dy_of(i + 1);
+#pragma unroll
+            for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, dyn));
+        }
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void danielsson3_warp(int16_t* __restrict__ dl, int w, int h, int d, int cw)
+{
+    const int lane = threadIdx.x & 31;
+    const int nseg = (w + S - 1) / S;
+    const bool active = lane < nseg;
+    const int n = active ? min(S, w - lane * S) : 0;
+    const long long x0 = (long long)lane * S;
+    const long long plane = (long long)w * h;
+    const int steps = 2 * (h - 1);
+    auto row_of = [&](int i) { return i < h - 1 ? i + 1 : 2 * h - 3 - i; };
+    auto dy_of = [&](int i) { return i < h - 1 ? -cw : cw; };
+    C3 P[S], C[S], Q[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = Q[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
+    for (int pass = 0; pass < 2; pass++) {
+        const int dz = pass == 0 ? -cw : +cw;
+        for (int k = 1; k < d; k++) {
+            const int z = pass == 0 ? k : d - 1 - k;
+            const int zp = pass == 0 ? z - 1 : z + 1;
+            const long long sb = z * plane, pb = (long long)zp * plane;
+            load_row<C3, S>(C, dl, sb + x0, n);
+            load_row<C3, S>(Q, dl, pb + x0, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) P[s] = closer(C[s], add(Q[s], 0, 0, dz));
+            store_row<C3, S>(dl, sb + x0, P, n);
+            if (h < 2) continue;
+            load_row<C3, S>(C, dl, sb + (long long)w + x0, n);
+            load_row<C3, S>(Q, dl, pb + (long long)w + x0, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) V[s] = closer(closer(C[s], add(Q[s], 0, 0, dz)), add(P[s], 0, -cw, 0));
+            for (int i = 0; i < steps; i++) {
+                const int y = row_of(i);
+                const bool more = i + 1 < steps;
+                const bool next_down = more && i + 1 < h - 1;
+                if (more) {
+                    const long long off = (long long)row_of(i + 1) * w + x0;
+                    load_row<C3, S>(C, dl, sb + off, n);
+                    if (next_down) load_row<C3, S>(Q, dl, pb + off, n);
+                }
+                row_pass_warp<C3, S, false, +1>(R, V, lane, nseg, n, cw, D, warp_round0_input<C3, S, +1>(V, n, lane));
+                row_pass_warp<C3, S, false, -1>(P, R, lane, nseg, n, cw, D, warp_round0_input<C3, S, -1>(R, n, lane));
+                store_row<C3, S>(dl, sb + (long long)y * w + x0, P, n);
+                if (more) {
+                    const int dyn = dy_of(i + 1);
+#pragma unroll
+                    for (int s = 0; s < S; s++) {
+                        C3 c = next_down ? closer(C[s], add(Q[s], 0, 0, dz)) : C[s];
+                        V[s] = closer(c, add(P[s], 0, dyn, 0));
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(32) k_danielsson2_w(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    danielsson2_warp<S>(dl, w, h, cw);
+}
+
+template <int S>
+__global__ void __launch_bounds__(32) k_danielsson3_w(int16_t* __restrict__ dl, int w, int h, int d, int cw)
+{
+    danielsson3_warp<S>(dl, w, h, d, cw);
+}
+
+template <int S>
+__global__ void __launch_bounds__(32) k_fastsweep2_w(uint32_t* __restrict__ dl, int w, int h, int cw)
+{
+    const int lane = threadIdx.x & 31;
+    const int nseg = (w + S - 1) / S;
+    const bool active = lane < nseg;
+    const int n = active ? min(S, w - lane * S) : 0;
+    const long long x0 = (long long)lane * S;
+    C2 P[S], C[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) P[s] = C[s] = V[s] = R[s] = D[s] = C2{0, 0};
+    if (h < 2) return;
+    for (int sweep = 0; sweep < 4; sweep++) {
+        const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1;
+        const int ox = -cw * dx, oy = -cw * dy;
+        const int y0 = dy > 0 ? 0 : h - 1;
+        const int pred = lane - dx;
+        const bool has_pred = active && pred >= 0 && pred < nseg;
+        const int src = pred < 0 ? 0 : (pred > 31 ? 31 : pred);
+        load_row<C2, S>(P, dl, (long long)y0 * w + x0, n);
+        load_row<C2, S>(C, dl, (long long)(y0 + dy) * w + x0, n);
+#pragma unroll
+        for (int s = 0; s < S; s++) V[s] = closer(C[s], add(P[s], 0, oy));
+        for (int j = 1; j < h; j++) {
+            const int y = y0 + j * dy;
+            const bool more = j + 1 < h;
+            if (more) load_row<C2, S>(C, dl, (long long)(y + dy) * w + x0, n);
+            // diagonal candidates from the previous row: own cells, then the predecessor's edge
+            C2 e;
+            if (dx > 0) {
+#pragma unroll
+                for (int s = 1; s < S; s++) D[s] = add(P[s - 1], ox, oy);
+                e = shfl_cell(0xFFFFFFFFu, seg_edge<C2, S, +1>(P, n), src);
+            } else {
+#pragma unroll
+                for (int s = 0; s + 1 < S; s++) D[s] = add(P[s + 1], ox, oy);
+                e = shfl_cell(0xFFFFFFFFu, seg_edge<C2, S, -1>(P, n), src);
+            }
+            if (has_pred) {
+                e = add(e, ox, oy);
+                if (dx > 0) D[0] = e;
+                else {
+#pragma unroll
+                    for (int s = 0; s < S; s++)
+                        if (s == n - 1) D[s] = e;
+                }
+            }
+            if (dx > 0)
+                row_pass_warp<C2, S, true, +1>(R, V, lane, nseg, n, cw, D, warp_round0_input<C2, S, +1>(V, n, lane));
+            else
+                row_pass_warp<C2, S, true, -1>(R, V, lane, nseg, n, cw, D, warp_round0_input<C2, S, -1>(V, n, lane));
+            store_row<C2, S>(dl, (long long)y * w + x0, R, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) {
+                P[s] = R[s];
+                if (more) V[s] = closer(C[s], add(P[s], 0, oy));
+            }
+        }
+    }
+}
+
 // --------------------------------------------------------------- launchers ----
 
 // cells per thread: aim for at most 256 threads (fewer warps at every barrier),
@@ -394,11 +562,44 @@ static int threads_for(int w, int s)
     return ((n + 31) / 32) * 32;
 }
 
+// The single-warp engines take rows up to 32 * 16 cells (2D) / 32 * 8 (3D).
+// Tuning value kWarpEngine selects them; 1/2/4/8 select the CTA engine with
+// that many cells per thread; 0 (untuned) picks the warp engine when it fits.
+constexpr int kWarpEngine = 32;
+
+static int warp_s(int w, int max_s)
+{
+    for (int s = 1; s <= max_s; s *= 2)
+        if (32 * s >= w) return s;
+    return 0;
+}
+
 void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st)
 {
-    const int s = tuned_s(dim == 2 ? kTuneDan2 : kTuneDan3, w, 512);
-    const int T = threads_for(w, s);
+    const int kind = dim == 2 ? kTuneDan2 : kTuneDan3;
+    const int tv = tune_get(kind, w);
+    const int ws = warp_s(w, dim == 2 ? 16 : 8);
     ProfScope ps("danielsson", st);
+    if (ws && (tv == kWarpEngine || tv == 0)) {
+#define DOL_DANW_CASE(SV)                                                                             \
+    case SV:                                                                                          \
+        if (dim == 2)                                                                                 \
+            k_danielsson2_w<SV><<<1, 32, 0, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);         \
+        else                                                                                          \
+            k_danielsson3_w<(SV > 8 ? 8 : SV)><<<1, 32, 0, st>>>(static_cast<int16_t*>(deltas), w, h, d, cw); \
+        return;
+        switch (ws) {
+            DOL_DANW_CASE(1)
+            DOL_DANW_CASE(2)
+            DOL_DANW_CASE(4)
+            DOL_DANW_CASE(8)
+            DOL_DANW_CASE(16)
+            default: break;
+        }
+#undef DOL_DANW_CASE
+    }
+    const int s = tuned_s(kind, w, 512);
+    const int T = threads_for(w, s);
 #define DOL_DAN_CASE(SV)                                                                              \
     case SV:                                                                                          \
         if (dim == 2)                                                                                 \
@@ -418,9 +619,26 @@ void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaS
 
 void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st)
 {
+    const int tv = tune_get(kTuneFs2, w);
+    const int ws = warp_s(w, 16);
+    ProfScope ps("fastsweep_2d", st);
+    if (ws && (tv == kWarpEngine || tv == 0)) {
+#define DOL_FSW_CASE(SV)                                                                              \
+    case SV:                                                                                          \
+        k_fastsweep2_w<SV><<<1, 32, 0, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);              \
+        return;
+        switch (ws) {
+            DOL_FSW_CASE(1)
+            DOL_FSW_CASE(2)
+            DOL_FSW_CASE(4)
+            DOL_FSW_CASE(8)
+            DOL_FSW_CASE(16)
+            default: break;
+        }
+#undef DOL_FSW_CASE
+    }
     const int s = tuned_s(kTuneFs2, w, 512);
     const int T = threads_for(w, s);
-    ProfScope ps("fastsweep_2d", st);
 #define DOL_FS_CASE(SV)                                                                                      \
     case SV:                                                                                                 \
         k_fastsweep2<SV><<<1, T, 0, st>>>(static_cast<uint32_t*>(deltas), w, h, cw);                         \

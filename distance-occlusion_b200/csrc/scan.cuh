@@ -174,3 +174,74 @@ __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t
 }
 
 }  // namespace dolk
+
+namespace dolk {
+
+// ---- single-warp form -----------------------------------------------------------
+// For rows of at most 32*S cells one warp holds the whole row and every
+// exchange is a shuffle: no shared memory, no CTA barrier.  Same rounds, same
+// jump rule, same exactness argument as row_pass; convergence is a warp vote.
+
+DOL_HD C2 shfl_cell(unsigned m, C2 c, int src)
+{
+#if defined(__CUDA_ARCH__)
+    return C2{__shfl_sync(m, c.x, src), __shfl_sync(m, c.y, src)};
+#else
+    (void)m; (void)src;
+    return c;
+#endif
+}
+DOL_HD C3 shfl_cell(unsigned m, C3 c, int src)
+{
+#if defined(__CUDA_ARCH__)
+    return C3{__shfl_sync(m, c.x, src), __shfl_sync(m, c.y, src), __shfl_sync(m, c.z, src)};
+#else
+    (void)m; (void)src;
+    return c;
+#endif
+}
+
+// The predecessor's boundary cell before the pass (round-0 input), from the
+// lane before (dir > 0) or after (dir < 0) in scan order.
+template <class Cell, int S, int dir>
+__device__ __forceinline__ Cell warp_round0_input(const Cell (&V)[S], int n, int lane)
+{
+    const Cell e = seg_edge<Cell, S, dir>(V, n);
+    return shfl_cell(0xFFFFFFFFu, e, dir > 0 ? (lane > 0 ? lane - 1 : 0) : (lane < 31 ? lane + 1 : 31));
+}
+
+template <class Cell, int S, bool kDiag, int dir>
+__device__ __forceinline__ void row_pass_warp(Cell (&R)[S], const Cell (&V)[S], int lane, int nseg, int n, int cw,
+                                              const Cell (&D)[S], Cell in0)
+{
+    const bool active = lane < nseg;
+    const int sigma = dir > 0 ? lane : nseg - 1 - lane;
+    const bool has_pred = active && sigma > 0;
+    const bool has_succ = active && sigma < nseg - 1;
+    Cell in = in0;
+    Cell succ_in = seg_edge<Cell, S, dir>(V, n);
+    for (int r = 0;; r++) {
+        const Cell out = seg_pass<Cell, S, kDiag, dir>(R, V, n, cw, in, has_pred, D);
+        const bool trans = has_pred && same(out, addx(in, -dir * cw * n));
+        const uint32_t nt = __ballot_sync(0xFFFFFFFFu, active && !trans);
+        const bool bad = has_succ && !same(succ_in, out);
+        if (!__any_sync(0xFFFFFFFFu, bad) || r > nseg + 2) break;
+        // nearest non-transparent lane before me in scan order (exists for has_pred)
+        int j = lane;
+        if (dir > 0) {
+            const uint32_t below = nt & ((1u << lane) - 1u);
+            if (below) j = 31 - __clz(below);
+        } else {
+            const uint32_t above = lane == 31 ? 0u : (nt & ~((2u << lane) - 1u));
+            if (above) j = __ffs(above) - 1;
+        }
+        const Cell src = shfl_cell(0xFFFFFFFFu, out, j);
+        if (has_pred) {
+            const int gap = (dir > 0 ? lane - j : j - lane) - 1;
+            in = addx(src, -dir * cw * S * gap);
+        }
+        succ_in = trans ? addx(in, -dir * cw * n) : out;
+    }
+}
+
+}  // namespace dolk

@@ -63,9 +63,11 @@ static std::vector<int> candidates(int kind, int w)
         case kTuneDan2:
         case kTuneFs2:
         case kTuneDan3: {
+            // CTA engine with 1/2/4/8 cells per thread, or (32) the single-warp engine
             std::vector<int> c;
             for (int s : {1, 2, 4, 8})
                 if ((w + s - 1) / s <= 512) c.push_back(s);
+            if (w <= (kind == kTuneDan3 ? 256 : 512)) c.push_back(32);
             return c;
         }
         case kTuneFs3: {

@@ -242,7 +242,7 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
    device and per size bucket (ceil(log2(w))); 0 = the built-in heuristic.
    dol_autotune times every candidate on a synthetic problem of the given shape
    (blocking; it allocates its own scratch) and keeps the fastest. */
-#define DOL_TUNE_DANIELSSON_2D 0   /* cells per thread: 1, 2, 4, 8 */
+#define DOL_TUNE_DANIELSSON_2D 0   /* CTA engine with 1, 2, 4, 8 cells per thread; 32 = single-warp engine */
 #define DOL_TUNE_DANIELSSON_3D 1
 #define DOL_TUNE_FASTSWEEP_2D  2
 #define DOL_TUNE_FASTSWEEP_3D  3

@@ -228,7 +228,38 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
         _config4(dol, torch, res, L, sp)
     if big and want("c3"):
         _config3(dol, torch, res, L, sp)
+    if only is not None and "c6" in only:
+        _sweep_variants(dol, torch, res, L, sp)
     return res
+
+
+def _sweep_variants(dol, torch, res, L, sp):
+    """Danielsson time per launch configuration (every value the tuner may
+    choose), on the 2D default image and on a 256^3 shape volume."""
+    out = {}
+    dims2 = (1024, 1024)
+    m2 = dol.add_points(np.zeros(dol.mask_words(*dims2), np.uint32), dims2, 100, 1)
+    md2 = torch.from_numpy(m2.view(np.int32)).cuda()
+    base2 = dol.init_deltas(md2, dims2)
+    work2 = base2.clone()
+    n = 256
+    dims3 = (n, n, n)
+    md3 = torch.empty(dol.mask_words(*dims3), dtype=torch.int32, device="cuda")
+    dol.check(L.dol_gen_shapes_3d(n, n, n, 32, 32, 4, 40, C.c_uint32(7), C.c_void_p(md3.data_ptr()), sp))
+    base3 = dol.init_border(md3, dims3)
+    work3 = base3.clone()
+    for kind, dims, base, work, cw, vals in ((0, dims2, base2, work2, 1, (1, 2, 4, 8)),
+                                             (1, dims3, base3, work3, 2, (1, 2, 4, 8, 32))):
+        for v in vals:
+            L.dol_tune_set(kind, dims[0], v)
+            def run():
+                work.copy_(base)
+                dol.danielsson(work, dims, cw)
+            run()
+            t = _ev_ms(torch, run, 1) - _ev_ms(torch, lambda: work.copy_(base), 1)
+            out[f"{'2d' if kind == 0 else '3d'}_{'warp' if v == 32 else 'cta_s' + str(v)}_ms"] = t
+        L.dol_tune_set(kind, dims[0], 0)
+    res["danielsson_variants"] = out
 
 
 def _config1(dol, torch, O, ref, res, dims):

@@ -621,7 +621,13 @@ dol_status dol_batch_prepare(int n, const dol_batch_item* items, void* workspace
         work[i] = it.d > 1 ? 4.0 * it.d * it.h + 1e-3 * it.w * it.h * it.d : 2.0 * it.h + 1e-3 * it.w * it.h;
         order[i] = i;
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    // items with rows over 256 cells (whole-CTA engine) first, then the
+    // one-warp items; each group by decreasing work
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const bool wa = items[a].w > 256, wb = items[b].w > 256;
+        if (wa != wb) return wa;
+        return work[a] > work[b];
+    });
     char* p = static_cast<char*>(workspace);
     cudaStream_t st = S(stream);
     cudaError_t e = cudaMemcpyAsync(p, items, (size_t)n * sizeof(dol_batch_item), cudaMemcpyHostToDevice, st);

@@ -776,6 +776,80 @@ __device__ __forceinline__ void signed_dist_cta(const uint32_t* mask, const P* d
     }
 }
 
+// warp-cooperative pieces for items whose rows fit one warp
+__device__ __forceinline__ void border2_warp(const uint32_t* mask, uint32_t* dl, int w, int h)
+{
+    const int lane = threadIdx.x & 31;
+    const int ws = words_per_row(w);
+    for (long long wid = lane; wid < (long long)ws * h; wid += 32) {
+        const int y = (int)(wid / ws), k = (int)(wid - (long long)y * ws);
+        Planes2 p = border2_word(w, h, mask, y, k);
+        const int n = min(32, w - 32 * k);
+        uint32_t* row = dl + (long long)y * w + 32 * k;
+        for (int b = 0; b < n; b++) row[b] = pack2(decode2(p, b));
+    }
+}
+
+__device__ __forceinline__ void border3_warp(const uint32_t* mask, int16_t* dl, int w, int h, int d)
+{
+    const int lane = threadIdx.x & 31;
+    const int ws = words_per_row(w);
+    const long long words = (long long)ws * h * d;
+    for (long long wid = lane; wid < words; wid += 32) {
+        const long long row = wid / ws;
+        const int k = (int)(wid - row * ws);
+        const int z = (int)(row / h), y = (int)(row - (long long)z * h);
+        Planes3 p = border3_word(w, h, d, mask, z, y, k);
+        const int n = min(32, w - 32 * k);
+        for (int b = 0; b < n; b++) cell_store(dl, row * w + 32 * k + b, decode3(p, b));
+    }
+}
+
+template <class Cell, class P>
+__device__ __forceinline__ void signed_dist_warp(const uint32_t* mask, const P* dl, float* out, int w, long long rows)
+{
+    const int lane = threadIdx.x & 31;
+    const int ws = words_per_row(w);
+    for (long long i = lane; i < rows * w; i += 32) {
+        const long long row = i / w;
+        const int x = (int)(i - row * w);
+        float r = __fdiv_rn(sqrtf((float)len(cell_load(dl, i))), 2.0f);
+        if ((mask[row * ws + (x >> 5)] >> (x & 31)) & 1u) r = -r;
+        out[i] = r;
+    }
+}
+
+// an item processed by one warp: rows of at most 256 cells
+__device__ __noinline__ void batch_item_warp(const BatchItemDev& b, const uint32_t* masks, unsigned char* deltas,
+                                             float* dist)
+{
+    const uint32_t* m = masks + b.mask_off;
+    if (b.d <= 1) {
+        uint32_t* dl = reinterpret_cast<uint32_t*>(deltas + b.delta_off);
+        border2_warp(m, dl, b.w, b.h);
+        __syncwarp();
+        if (b.w <= 64) danielsson2_warp<2>(dl, b.w, b.h, 2);
+        else if (b.w <= 128) danielsson2_warp<4>(dl, b.w, b.h, 2);
+        else danielsson2_warp<8>(dl, b.w, b.h, 2);
+        __syncwarp();
+        if (dist && b.dist_off >= 0) signed_dist_warp<C2>(m, dl, dist + b.dist_off, b.w, b.h);
+    } else {
+        int16_t* dl = reinterpret_cast<int16_t*>(deltas + b.delta_off);
+        border3_warp(m, dl, b.w, b.h, b.d);
+        __syncwarp();
+        if (b.w <= 64) danielsson3_warp<2>(dl, b.w, b.h, b.d, 2);
+        else if (b.w <= 128) danielsson3_warp<4>(dl, b.w, b.h, b.d, 2);
+        else danielsson3_warp<8>(dl, b.w, b.h, b.d, 2);
+        __syncwarp();
+        if (dist && b.dist_off >= 0) signed_dist_warp<C3>(m, dl, dist + b.dist_off, b.w, (long long)b.h * b.d);
+    }
+}
+
+// Items are ordered with the wide ones (rows > 256 cells: whole-CTA engine)
+// first, largest work first, then the narrow ones.  A CTA draws items one at a
+// time while they are wide; the first narrow item it draws switches it to
+// per-warp draining: each warp takes narrow items on its own until the queue
+// is empty.
 template <int S>
 __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restrict__ items, const int* __restrict__ order,
                                                    int n, const uint32_t* __restrict__ masks,
@@ -785,13 +859,28 @@ __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restric
     __shared__ ScanShared<C3> sh3;   // the larger of the two; the 2D engine reuses its storage
     __shared__ int s_item;
     ScanShared<C2>& sh2 = *reinterpret_cast<ScanShared<C2>*>(&sh3);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();
-        if (it >= n) break;
+        if (it >= n) return;
         const BatchItemDev b = items[order[it]];
+        if (b.w <= 256) {
+            // narrow from here on: warp 0 takes this item, every warp then drains the queue
+            int mine = warp == 0 ? it : -1;
+            for (;;) {
+                if (mine < 0) {
+                    int v = 0;
+                    if (lane == 0) v = atomicAdd(counter, 1);
+                    mine = __shfl_sync(0xFFFFFFFFu, v, 0);
+                    if (mine >= n) return;
+                }
+                batch_item_warp(items[order[mine]], masks, deltas, dist);
+                mine = -1;
+            }
+        }
         const uint32_t* m = masks + b.mask_off;
         if (b.d <= 1) {
             uint32_t* dl = reinterpret_cast<uint32_t*>(deltas + b.delta_off);

@@ -226,6 +226,8 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
         _config2(dol, torch, O, ref, res, L, sp)
     if want("c4"):
         _config4(dol, torch, res, L, sp)
+    if want("c5"):
+        _config5(dol, torch, res)
     if big and want("c3"):
         _config3(dol, torch, res, L, sp)
     if only is not None and "c6" in only:
@@ -248,17 +250,23 @@ def _sweep_variants(dol, torch, res, L, sp):
     dol.check(L.dol_gen_shapes_3d(n, n, n, 32, 32, 4, 40, C.c_uint32(7), C.c_void_p(md3.data_ptr()), sp))
     base3 = dol.init_border(md3, dims3)
     work3 = base3.clone()
+    rows_kind = 8
     for kind, dims, base, work, cw, vals in ((0, dims2, base2, work2, 1, (1, 2, 4, 8)),
                                              (1, dims3, base3, work3, 2, (1, 2, 4, 8, 32))):
-        for v in vals:
-            L.dol_tune_set(kind, dims[0], v)
-            def run():
-                work.copy_(base)
-                dol.danielsson(work, dims, cw)
-            run()
-            t = _ev_ms(torch, run, 1) - _ev_ms(torch, lambda: work.copy_(base), 1)
-            out[f"{'2d' if kind == 0 else '3d'}_{'warp' if v == 32 else 'cta_s' + str(v)}_ms"] = t
-        L.dol_tune_set(kind, dims[0], 0)
+        tag = '2d' if kind == 0 else '3d'
+        for rows in (4, 8, 16, 32, 65536):
+            L.dol_tune_set(rows_kind, dims[0], rows)
+            for v in (vals if rows == 65536 else (1, 2, 4)):
+                L.dol_tune_set(kind, dims[0], v)
+                def run():
+                    work.copy_(base)
+                    dol.danielsson(work, dims, cw)
+                run()
+                t = _ev_ms(torch, run, 1) - _ev_ms(torch, lambda: work.copy_(base), 1)
+                eng = 'warp' if v == 32 else 'cta_s' + str(v)
+                out[f"{tag}_{'serial' if rows == 65536 else 'rows' + str(rows)}_{eng}_ms"] = t
+            L.dol_tune_set(kind, dims[0], 0)
+        L.dol_tune_set(rows_kind, dims[0], 0)
     res["danielsson_variants"] = out
 
 
@@ -362,6 +370,38 @@ def _config4(dol, torch, res, L, sp):
         "looped_masks_per_s": len(sample) / t_loop * 1e3,
         "batched_over_looped": (nitems / t_batch) / (len(sample) / t_loop),
         "path": "batched: one persistent launch replayed from a CUDA graph; looped: dol_sdf_* per item"}
+
+
+def _config5(dol, torch, res):
+    """Float sites: forward (seed, plain delta method, |p - site|) against
+    forward + loss gradient + backward, 4096 sites (seed 11) on 512^2 and
+    128^3, targets from the sites jittered by N(0, 0.5)."""
+    out = {}
+    for dims in ((512, 512), (128, 128, 128)):
+        sites = dol.gen_sites(4096, dims, 11)
+        rng = np.random.default_rng(11)
+        jit = np.clip(sites + rng.normal(0, 0.5, sites.shape), 0, np.array(dims, np.float32) - 1e-3)
+        s = torch.from_numpy(sites).cuda()
+        sj = torch.from_numpy(jit.astype(np.float32)).cuda()
+        cells = int(np.prod(dims))
+        for meth in ("danielsson", "jumpflood"):
+            dt, _, _ = dol.sites_forward(sj, dims, meth)
+
+            def fwd(meth=meth):
+                return dol.sites_forward(s, dims, meth)
+
+            def fwd_bwd(meth=meth):
+                d, own, _ = dol.sites_forward(s, dims, meth)
+                return dol.sites_backward(own, s, 2.0 * (d - dt), dims)
+            fwd_bwd()
+            torch.cuda.synchronize()
+            tf = _ev_ms(torch, fwd, 3)
+            tfb = _ev_ms(torch, fwd_bwd, 3)
+            key = f"{'x'.join(map(str, dims))}_{meth}"
+            out[key] = {"fwd_ms": tf, "fwd_bwd_ms": tfb, "fwd_bwd_over_fwd": tfb / tf,
+                        "fwd_bwd_gvox_per_s": cells / tfb / 1e6}
+    res["sites_4096"] = {"workload": "4096 float sites (seed 11), loss sum (d - d_t)^2, d_t from sites + N(0,0.5)",
+                         **out}
 
 
 def _config3(dol, torch, res, L, sp):

@@ -361,7 +361,10 @@ dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* str
     DOL_TRY(check_cw(cw));
     DOL_TRY(check_sweep_width(w));
     DOL_TRY(check_dev_ptr(deltas, "deltas"));
-    launch_danielsson(2, deltas, w, h, 1, cw, S(stream));
+    Workspace ws;
+    const size_t need = danielsson_workspace_bytes(2, w, h, 1);
+    if (get_workspace(ws, nullptr, 0, need, S(stream)) != DOL_OK) ws.ptr = nullptr;   // serial engine needs none
+    run_danielsson(2, deltas, w, h, 1, cw, ws.ptr, need, ds->err_dev, S(stream));
     return launched("danielsson_2d");
 }
 
@@ -373,7 +376,10 @@ dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, vo
     DOL_TRY(check_cw(cw));
     DOL_TRY(check_sweep_width(w));
     DOL_TRY(check_dev_ptr(deltas, "deltas"));
-    launch_danielsson(3, deltas, w, h, d, cw, S(stream));
+    Workspace ws;
+    const size_t need = danielsson_workspace_bytes(3, w, h, d);
+    if (get_workspace(ws, nullptr, 0, need, S(stream)) != DOL_OK) ws.ptr = nullptr;   // serial engine needs none
+    run_danielsson(3, deltas, w, h, d, cw, ws.ptr, need, ds->err_dev, S(stream));
     return launched("danielsson_3d");
 }
 
@@ -531,6 +537,7 @@ size_t dol_sdf_workspace_size(int w, int h, int d, int method)
     size_t b = align256(cells * cb);                       // deltas, when the caller passes none
     if (method == DOL_JUMPFLOOD) b += align256(cells * cb);  // ping-pong buffer
     if (method == DOL_FASTSWEEP && dim == 3) b += align256(fastsweep3_workspace_bytes(w, h, d));
+    if (method == DOL_DANIELSSON) b += align256(danielsson_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
     return b;
 }
 
@@ -568,7 +575,8 @@ static dol_status sdf_common(int dim, int w, int h, int d, const uint32_t* mask,
     p += align256(cells * cb);
     launch_init_border(dim, mask, dl, w, h, d, st);
     if (method == DOL_DANIELSSON) {
-        launch_danielsson(dim, dl, w, h, d, 2, st);
+        run_danielsson(dim, dl, w, h, d, 2, p, danielsson_workspace_bytes(dim, w, h, dim == 3 ? d : 1), ds->err_dev,
+                       st);
     } else if (method == DOL_FASTSWEEP) {
         if (dim == 2)
             launch_fastsweep_2d(dl, w, h, 2, st);

@@ -26,7 +26,18 @@ int set_error(int s, const char* fmt, ...);
 
 // launch-configuration table (tune.cu); values are family specific, 0 = use
 // the launcher's heuristic.  The order matches the DOL_TUNE_* constants.
-enum TuneKind { kTuneDan2 = 0, kTuneDan3, kTuneFs2, kTuneFs3, kTuneJfa2, kTuneJfa3, kTuneBatch, kTuneEdt, kTuneKinds };
+enum TuneKind {
+    kTuneDan2 = 0,
+    kTuneDan3,
+    kTuneFs2,
+    kTuneFs3,
+    kTuneJfa2,
+    kTuneJfa3,
+    kTuneBatch,
+    kTuneEdt,
+    kTuneDanRows,
+    kTuneKinds
+};
 int tune_get(int kind, int w);
 void tune_put(int kind, int w, int value);
 
@@ -63,6 +74,19 @@ void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* 
 // k_sweep.cu -- Danielsson / FastSweep; `err` is a device int that receives a
 // non-zero code if a bounded wait gives up
 void launch_danielsson(int dim, void* deltas, int w, int h, int d, int cw, cudaStream_t st);
+// k_dan_blocks.cu -- Danielsson as a fixed-point iteration over blocks of R
+// rows (exact); false if the launch could not be made (the caller then runs
+// the serial engine)
+constexpr int kDanSerial = 65536;   // kTuneDanRows value that selects the serial engine
+int dan_blocks_rows(int dim, int w, int h, int d);
+size_t dan_blocks_workspace_bytes(int dim, int w, int h, int d, int R);
+bool launch_danielsson_blocks(int dim, void* deltas, int w, int h, int d, int cw, int R, void* ws, int* err,
+                              cudaStream_t st);
+// the Danielsson entry used by the C ABI: the block schedule when its
+// workspace is given and the shape calls for it, else the serial engine
+size_t danielsson_workspace_bytes(int dim, int w, int h, int d);
+void run_danielsson(int dim, void* deltas, int w, int h, int d, int cw, void* ws, size_t ws_bytes, int* err,
+                    cudaStream_t st);
 void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st);
 size_t fastsweep3_workspace_bytes(int w, int h, int d);
 // batched signed Danielsson; items: device array of dol_batch_item (40 bytes)

@@ -40,12 +40,12 @@ namespace dolk {
 
 constexpr int kMaxScanThreads = 512;
 
-template <class Cell>
+template <class Cell, int N = kMaxScanThreads>
 struct ScanShared {
-    Cell out[2][kMaxScanThreads];     // segment outputs, by round parity
-    uint32_t nt[2][32];               // per warp: ballot of non-transparent segments, by round parity
-    Cell guess[2][kMaxScanThreads];   // boundary cells published for the next pass, by pass parity
-    Cell edge[2][kMaxScanThreads];    // FastSweep 2D: each segment's boundary cell of the previous row
+    Cell out[2][N];     // segment outputs, by round parity
+    uint32_t nt[2][32]; // per warp: ballot of non-transparent segments, by round parity
+    Cell guess[2][N];   // boundary cells published for the next pass, by pass parity
+    Cell edge[2][N];    // FastSweep 2D: each segment's boundary cell of the previous row
 };
 
 // Load/store helpers for row cells.  2D cells are one uint32; 3D cells three int16.
@@ -113,9 +113,9 @@ __device__ __forceinline__ Cell seg_pass(Cell (&R)[S], const Cell (&V)[S], int n
 // after every round, before the round's barrier: the caller uses it to post
 // what the NEXT pass needs from this thread, so the final round's post is
 // visible to all threads when this function returns.
-template <class Cell, int S, bool kDiag, int dir, class Pub>
+template <class Cell, int S, bool kDiag, int dir, class Pub, int N>
 __device__ __forceinline__ void row_pass(Cell (&R)[S], const Cell (&V)[S], int t, int nseg, int n, int cw,
-                                         ScanShared<Cell>& sh, const Cell (&D)[S], Cell in0, Pub&& publish)
+                                         ScanShared<Cell, N>& sh, const Cell (&D)[S], Cell in0, Pub&& publish)
 {
     const int lane = t & 31, wi = t >> 5;
     const bool active = t < nseg;

@@ -80,6 +80,7 @@ static std::vector<int> candidates(int kind, int w)
         case kTuneJfa3: return {2, 4, 8, 16};
         case kTuneBatch: return {4, 8};
         case kTuneEdt: return {256, 512};
+        case kTuneDanRows: return {4, 8, 16, 32, kDanSerial};
     }
     return {};
 }
@@ -153,7 +154,8 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     if (w < 1 || h < 1 || d < 1) return (dol_status)set_error(DOL_ERR_INVALID_ARG, "empty shape");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (kind == kTuneBatch) return tune_batch(st);
-    const bool vol = kind == kTuneDan3 || kind == kTuneFs3 || kind == kTuneJfa3 || kind == kTuneEdt;
+    const bool vol = kind == kTuneDan3 || kind == kTuneFs3 || kind == kTuneJfa3 || kind == kTuneEdt ||
+                     (kind == kTuneDanRows && d > 1);
     // a bounded synthetic problem of the caller's row / line shape
     int tw = w, th = h, td = vol ? d : 1;
     if (kind == kTuneDan2 || kind == kTuneFs2) th = h < 256 ? h : 256;
@@ -162,7 +164,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
         td = d < 8 ? d : 8;
     }
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);
-    if (kind == kTuneJfa3 || kind == kTuneEdt) {
+    if (kind == kTuneJfa3 || kind == kTuneEdt || kind == kTuneDanRows) {
         while ((long long)tw * th * td > (1LL << 26) && td > 1) td = (td + 1) / 2;
     }
     const long long cells = (long long)tw * th * td;
@@ -183,7 +185,9 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     }
     void *dm = nullptr, *dl = nullptr, *tmp = nullptr, *ws = nullptr;
     const size_t cell_bytes = vol ? 6 : 4;
-    size_t ws_bytes = kind == kTuneEdt ? edt_workspace_bytes(3, tw, th, td) : fastsweep3_workspace_bytes(tw, th, td);
+    size_t ws_bytes = kind == kTuneEdt       ? edt_workspace_bytes(3, tw, th, td)
+                      : kind == kTuneDanRows ? dan_blocks_workspace_bytes(vol ? 3 : 2, tw, th, td, 1)
+                                             : fastsweep3_workspace_bytes(tw, th, td);
     bool ok = cudaMallocAsync(&dm, mwords * 4, st) == cudaSuccess &&
               cudaMallocAsync(&dl, (size_t)cells * (kind == kTuneEdt ? 4 : cell_bytes), st) == cudaSuccess &&
               cudaMallocAsync(&tmp, (size_t)cells * cell_bytes, st) == cudaSuccess &&
@@ -225,6 +229,10 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
             case kTuneEdt:
                 launch_edt_mask(3, static_cast<uint32_t*>(dm), static_cast<float*>(dl), tw, th, td, DOL_EDT_SIGNED, ws,
                                 err, st);
+                break;
+            case kTuneDanRows:
+                launch_init_border(dim, static_cast<uint32_t*>(dm), dl, tw, th, td, st);
+                run_danielsson(dim, dl, tw, th, td, 2, ws, ws_bytes, err, st);
                 break;
             case kTuneBatch:
                 break;

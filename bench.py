@@ -231,42 +231,67 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
     if big and want("c3"):
         _config3(dol, torch, res, L, sp)
     if only is not None and "c6" in only:
-        _sweep_variants(dol, torch, res, L, sp)
+        _sweep_variants(dol, torch, res, L, sp, big)
     return res
 
 
-def _sweep_variants(dol, torch, res, L, sp):
-    """Danielsson time per launch configuration (every value the tuner may
-    choose), on the 2D default image and on a 256^3 shape volume."""
+def _sweep_variants(dol, torch, res, L, sp, big=True):
+    """Danielsson time per launch configuration of the block schedule (rows
+    per block, slices per block, cells per thread) and of the serial engine,
+    on the 2D default image, a 256^3 shape volume and the 1024^3 noise
+    volume."""
     out = {}
+    ROWS, SLICES, DAN2, DAN3 = 8, 9, 0, 1
     dims2 = (1024, 1024)
     m2 = dol.add_points(np.zeros(dol.mask_words(*dims2), np.uint32), dims2, 100, 1)
     md2 = torch.from_numpy(m2.view(np.int32)).cuda()
     base2 = dol.init_deltas(md2, dims2)
     work2 = base2.clone()
+
+    def timed(work, base, dims, cw, reps=1):
+        def run():
+            work.copy_(base)
+            dol.danielsson(work, dims, cw)
+        run()
+        return _ev_ms(torch, run, reps) - _ev_ms(torch, lambda: work.copy_(base), reps)
+
+    for rows in (8, 16, 32, 64, 128, 65536):
+        L.dol_tune_set(ROWS, 1024, rows)
+        out[f"2d_1024_rows{rows}_ms"] = timed(work2, base2, dims2, 1, 3)
+    L.dol_tune_set(ROWS, 1024, 0)
+
     n = 256
     dims3 = (n, n, n)
     md3 = torch.empty(dol.mask_words(*dims3), dtype=torch.int32, device="cuda")
     dol.check(L.dol_gen_shapes_3d(n, n, n, 32, 32, 4, 40, C.c_uint32(7), C.c_void_p(md3.data_ptr()), sp))
     base3 = dol.init_border(md3, dims3)
     work3 = base3.clone()
-    rows_kind = 8
-    for kind, dims, base, work, cw, vals in ((0, dims2, base2, work2, 1, (1, 2, 4, 8)),
-                                             (1, dims3, base3, work3, 2, (1, 2, 4, 8, 32))):
-        tag = '2d' if kind == 0 else '3d'
-        for rows in (4, 8, 16, 32, 65536):
-            L.dol_tune_set(rows_kind, dims[0], rows)
-            for v in (vals if rows == 65536 else (1, 2, 4)):
-                L.dol_tune_set(kind, dims[0], v)
-                def run():
-                    work.copy_(base)
-                    dol.danielsson(work, dims, cw)
-                run()
-                t = _ev_ms(torch, run, 1) - _ev_ms(torch, lambda: work.copy_(base), 1)
-                eng = 'warp' if v == 32 else 'cta_s' + str(v)
-                out[f"{tag}_{'serial' if rows == 65536 else 'rows' + str(rows)}_{eng}_ms"] = t
-            L.dol_tune_set(kind, dims[0], 0)
-        L.dol_tune_set(rows_kind, dims[0], 0)
+    for rows in (4, 8, 16, 32):
+        L.dol_tune_set(ROWS, n, rows)
+        for z in (1, 2, 4, 8, 16, 32, 64, 0):
+            L.dol_tune_set(SLICES, n, z)
+            out[f"3d_256_rows{rows}_slices{z or 'auto'}_ms"] = timed(work3, base3, dims3, 2)
+    L.dol_tune_set(ROWS, n, 0)
+    L.dol_tune_set(SLICES, n, 0)
+    for s_ in (1, 2, 4):
+        L.dol_tune_set(DAN3, n, s_)
+        out[f"3d_256_auto_s{s_}_ms"] = timed(work3, base3, dims3, 2)
+    L.dol_tune_set(DAN3, n, 0)
+    del work3, base3
+    if big:
+        side = 1024
+        mdv = torch.empty(dol.mask_words(side, side, side), dtype=torch.int32, device="cuda")
+        dol.check(L.dol_gen_value_noise_3d(side, side, side, SPACING, C.c_uint32(SEED), C.c_void_p(mdv.data_ptr()), sp))
+        dv = torch.empty((side, side, side, 3), dtype=torch.int16, device="cuda")
+        for rows, z in ((8, 0), (8, 32), (8, 64), (8, 128), (8, 256), (16, 0), (4, 0)):
+            L.dol_tune_set(ROWS, side, rows)
+            L.dol_tune_set(SLICES, side, z)
+            dol.init_border(mdv, (side,) * 3, out=dv)
+            torch.cuda.synchronize()
+            out[f"3d_1024_rows{rows}_slices{z or 'auto'}_ms"] = _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)
+        L.dol_tune_set(ROWS, side, 0)
+        L.dol_tune_set(SLICES, side, 0)
+        del dv, mdv
     res["danielsson_variants"] = out
 
 

@@ -629,11 +629,12 @@ dol_status dol_batch_prepare(int n, const dol_batch_item* items, void* workspace
         work[i] = it.d > 1 ? 4.0 * it.d * it.h + 1e-3 * it.w * it.h * it.d : 2.0 * it.h + 1e-3 * it.w * it.h;
         order[i] = i;
     }
-    // items with rows over 256 cells (whole-CTA engine) first, then the
-    // one-warp items; each group by decreasing work
+    // whole-CTA items first (volumes, then images with rows over 256 cells),
+    // then the one-warp images; each group by decreasing work
+    auto group = [&](int i) { return items[i].d > 1 ? 0 : (items[i].w > 256 ? 1 : 2); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        const bool wa = items[a].w > 256, wb = items[b].w > 256;
-        if (wa != wb) return wa;
+        const int ga = group(a), gb = group(b);
+        if (ga != gb) return ga < gb;
         return work[a] > work[b];
     });
     char* p = static_cast<char*>(workspace);

@@ -76,7 +76,14 @@ struct DanBlk {
     int* wl[2];            // work lists by round parity
     unsigned* ctl;         // [0],[1] work-list sizes, [2] work counter, [3],[4] grid barrier, [5] rounds used
     int* err;
-    int w, h, d, R, nc, cw, dir, zfix, nblocks, max_rounds;
+    int w, h, d, R, nc, cw;
+    int dir;      // +1: slices zfirst, zfirst+1, ...; -1: downwards
+    int zfirst;   // first slice of the phase's chain (the slice before it keeps its input)
+    int nchain;   // slices in the chain (2D: 1)
+    int Z;        // slices per block
+    int nk;       // blocks along the chain: ceil(nchain / Z)
+    int nblocks;  // nk * nc
+    int max_rounds;
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -117,11 +124,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int
 }
 
 // bits of DanBlk::chg
-constexpr int kChgRows = 1;    // some output row changed  -> block (z+dir, c)
-constexpr int kChgFirst = 2;   // row y0 changed           -> block (z, c-1)
-constexpr int kChgDown = 4;    // the down-sweep row y1-1  -> block (z, c+1)
+constexpr int kChgLast = 1;    // a row of the block's last slice changed  -> block (k+1, c)
+constexpr int kChgFirst = 2;   // row y0 of some slice changed             -> block (k, c-1)
+constexpr int kChgDown = 4;    // the down-sweep row y1-1 of some slice    -> block (k, c+1)
+constexpr int kChgAny = 8;     // any output changed: the block's version flips
 
-// One block: rows y0..y1-1 of slice z, T threads of S cells each.
+// One block: rows y0..y1-1 of Z consecutive slices (in the phase's order),
+// T threads of S cells each.
 template <class Cell, int kDim, int S>
 __device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cell, kBlkThreads>& sh, int* s_chg)
 {
@@ -133,33 +142,21 @@ __device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cel
     const bool active = t < nseg;
     const int n = active ? min(S, w - t * S) : 0;
     const long long x0 = (long long)t * S;
-    const int z = kDim == 3 ? b / p.nc : 0;
-    const int c = b - z * p.nc;
+    const int k = b / p.nc;
+    const int c = b - k * p.nc;
     const int y0 = c * p.R, y1 = min(y0 + p.R, h), L = y1 - y0;
-    const long long plane = (long long)w * h, sb = (long long)z * plane;
+    const long long plane = (long long)w * h;
     const P* A = static_cast<const P*>(p.A);
     auto ver = [&](int v) -> const P* { return v == 2 ? A : static_cast<const P*>(p.V[v]); };
     const int vo = __ldcg(p.lat + b), vn = vo == 0 ? 1 : 0;
     const P* oldv = ver(vo);
     P* out = static_cast<P*>(p.V[vn]);
-    const P* zin = nullptr;
-    int dz = 0;
-    if (kDim == 3) {
-        const int zp = z - p.dir;
-        zin = ver(__ldcg(p.lat + (long long)zp * p.nc + c)) + IO::kWords * (long long)zp * plane;
-        dz = -p.dir * cw;
-    }
-    const P* gd = nullptr;   // row y0-1 after the down sweep
-    if (c > 0) {
-        const int v = __ldcg(p.lat + b - 1);
-        gd = v == 2 ? A + IO::kWords * (sb + (long long)(y0 - 1) * w)
-                    : static_cast<const P*>(p.DB[v]) + IO::kWords * (long long)(b - 1) * w;
-    }
-    const P* gu = nullptr;   // row y1 after the up sweep
-    if (y1 < h) gu = ver(__ldcg(p.lat + b + 1)) + IO::kWords * (sb + (long long)y1 * w);
-    const P* dbo = vo == 2 ? A + IO::kWords * (sb + (long long)(y1 - 1) * w)
-                           : static_cast<const P*>(p.DB[vo]) + IO::kWords * (long long)b * w;
-    P* dbn = static_cast<P*>(p.DB[vn]) + IO::kWords * (long long)b * w;
+    // neighbour blocks' versions (fixed for the whole round)
+    const int vd = c > 0 ? __ldcg(p.lat + b - 1) : 2;
+    const int vu = y1 < h ? __ldcg(p.lat + b + 1) : 2;
+    const int vz = (kDim == 3 && k > 0) ? __ldcg(p.lat + b - p.nc) : 2;
+    const int dz = kDim == 3 ? -p.dir * cw : 0;
+    const int pos0 = k * p.Z, nsl = min(p.Z, p.nchain - pos0);
 
     auto ldrow = [&](Cell (&dst)[S], const P* base, long long first) {
 #pragma unroll
@@ -182,111 +179,129 @@ __device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cel
 #pragma unroll
     for (int s = 0; s < S; s++) Pr[s] = V[s] = Rr[s] = D[s] = Cn[s] = Qn[s] = Cell{};
     int bits = 0;
-
-    // row y0 before its x passes
-    ldrow(Cn, A, sb + (long long)y0 * w + x0);
-    if (kDim == 3) ldrow(Qn, zin, (long long)y0 * w + x0);
-#pragma unroll
-    for (int s = 0; s < S; s++) V[s] = Cn[s];
-    if (kDim == 3) {
-#pragma unroll
-        for (int s = 0; s < S; s++) V[s] = zpull(Cn[s], Qn[s]);
-    }
-    if (gd) {
-        ldrow(Qn, gd, x0);
-#pragma unroll
-        for (int s = 0; s < S; s++) V[s] = closer(V[s], yshift(Qn[s], -cw));
-    }
     int g = 0;
-    if (active) sh.guess[g][t] = seg_edge<Cell, S, +1>(V, n);
-    __syncthreads();
 
-    for (int i = 0; i < 2 * L; i++) {
-        const bool down = i < L;
-        const int y = down ? y0 + i : y1 - 1 - (i - L);
-        const bool pass = down ? y > 0 : y < h - 1;
-        const int nx = i + 1;                     // next step
-        const bool more = nx < 2 * L;
-        const bool nx_down = nx < L;
-        const bool nx_turn = nx == L;             // first up step: base = this result, candidate = U
-        const bool has_u = gu != nullptr;
-        // prefetch what the next step needs
-        if (more) {
-            if (nx_down) {
-                ldrow(Cn, A, sb + (long long)(y + 1) * w + x0);
-                if (kDim == 3) ldrow(Qn, zin, (long long)(y + 1) * w + x0);
-            } else if (nx_turn) {
-                if (has_u) ldrow(Cn, gu, x0);
-            } else {
-                ldrow(Cn, out, sb + (long long)(y - 1) * w + x0);   // its down-sweep result
-            }
+    for (int j = 0; j < nsl; j++) {
+        const int z = p.zfirst + p.dir * (pos0 + j);
+        const long long sb = (long long)z * plane;
+        const bool last = j == nsl - 1;
+        // the previous slice after its sweep: this block's own output, or the
+        // block before in z (or the fixed slice, which keeps the input)
+        const P* zin = nullptr;
+        if (kDim == 3) zin = (j > 0 ? static_cast<const P*>(out) : ver(vz)) + IO::kWords * (sb - p.dir * plane);
+        const long long dbi = ((long long)z * p.nc + c) * w;   // this slice's down-boundary row slot
+        const P* gd = nullptr;   // row y0-1 after the down sweep
+        if (c > 0)
+            gd = vd == 2 ? A + IO::kWords * (sb + (long long)(y0 - 1) * w)
+                         : static_cast<const P*>(p.DB[vd]) + IO::kWords * (dbi - w);
+        const P* gu = nullptr;   // row y1 after the up sweep
+        if (y1 < h) gu = ver(vu) + IO::kWords * (sb + (long long)y1 * w);
+        const P* dbo = vo == 2 ? A + IO::kWords * (sb + (long long)(y1 - 1) * w)
+                               : static_cast<const P*>(p.DB[vo]) + IO::kWords * dbi;
+        P* dbn = static_cast<P*>(p.DB[vn]) + IO::kWords * dbi;
+
+        // row y0 before its x passes
+        ldrow(Cn, A, sb + (long long)y0 * w + x0);
+        if (kDim == 3) ldrow(Qn, zin, (long long)y0 * w + x0);
+#pragma unroll
+        for (int s = 0; s < S; s++) V[s] = kDim == 3 ? zpull(Cn[s], Qn[s]) : Cn[s];
+        if (gd) {
+            ldrow(Qn, gd, x0);
+#pragma unroll
+            for (int s = 0; s < S; s++) V[s] = closer(V[s], yshift(Qn[s], -cw));
         }
-        // the next step's row before its x passes, from this step's result X
-        auto next_edge = [&](const Cell (&X)[S]) -> Cell {
-            const Cell e = seg_edge<Cell, S, +1>(X, n);
-            if (nx_down) {
-                const Cell cb = kDim == 3 ? zpull(seg_edge<Cell, S, +1>(Cn, n), seg_edge<Cell, S, +1>(Qn, n))
-                                          : seg_edge<Cell, S, +1>(Cn, n);
-                return closer(cb, yshift(e, -cw));
-            }
-            if (nx_turn) return has_u ? closer(e, yshift(seg_edge<Cell, S, +1>(Cn, n), cw)) : e;
-            return closer(seg_edge<Cell, S, +1>(Cn, n), yshift(e, cw));
-        };
-        if (pass) {
-            const Cell in0 = (active && t > 0) ? sh.guess[g][t - 1] : V[0];
-            row_pass<Cell, S, false, +1>(Rr, V, t, nseg, n, cw, sh, D, in0, [&](const Cell (&X)[S]) {
-                if (active) sh.guess[g ^ 1][t] = X[0];
-            });
-            g ^= 1;
-            const Cell in1 = (active && t + 1 < nseg) ? sh.guess[g][t + 1] : Rr[0];
-            row_pass<Cell, S, false, -1>(Pr, Rr, t, nseg, n, cw, sh, D, in1, [&](const Cell (&X)[S]) {
-                if (more && active) sh.guess[g ^ 1][t] = next_edge(X);
-            });
-            g ^= 1;
-        } else {
-#pragma unroll
-            for (int s = 0; s < S; s++) Pr[s] = V[s];
-            if (more && active) sh.guess[g][t] = next_edge(Pr);
-            __syncthreads();
-        }
-        const long long rf = sb + (long long)y * w + x0;
-        if (down) {
-            strow(out, rf, Pr);
-            if (i == L - 1) {
-                Cell O[S];
-#pragma unroll
-                for (int s = 0; s < S; s++) O[s] = Cell{};
-                ldrow(O, dbo, x0);
-#pragma unroll
-                for (int s = 0; s < S; s++)
-                    if (s < n && !same(O[s], Pr[s])) bits |= kChgDown;
-                strow(dbn, x0, Pr);
-            }
-        } else {
+        __syncthreads();   // the previous slice's last pass may still read the guess slots
+        if (active) sh.guess[g][t] = seg_edge<Cell, S, +1>(V, n);
+        __syncthreads();
+
+        for (int i = 0; i < 2 * L; i++) {
+            const bool down = i < L;
+            const int y = down ? y0 + i : y1 - 1 - (i - L);
+            const bool pass = down ? y > 0 : y < h - 1;
+            const int nx = i + 1;                     // next step
+            const bool more = nx < 2 * L;
+            const bool nx_down = nx < L;
+            const bool nx_turn = nx == L;             // first up step: base = this result, candidate = U
+            const bool has_u = gu != nullptr;
+            const long long rf = sb + (long long)y * w + x0;
+            // the old output this step's result is compared with, loaded
+            // before the passes so its latency hides behind them
             Cell O[S];
 #pragma unroll
             for (int s = 0; s < S; s++) O[s] = Cell{};
-            ldrow(O, oldv, rf);
-            bool diff = false;
-#pragma unroll
-            for (int s = 0; s < S; s++)
-                if (s < n && !same(O[s], Pr[s])) diff = true;
-            if (diff) bits |= (y == y0) ? (kChgRows | kChgFirst) : kChgRows;
-            strow(out, rf, Pr);
-        }
-        if (more) {
-            if (nx_down) {
-#pragma unroll
-                for (int s = 0; s < S; s++) {
-                    const Cell cb = kDim == 3 ? zpull(Cn[s], Qn[s]) : Cn[s];
-                    V[s] = closer(cb, yshift(Pr[s], -cw));
+            if (!down)
+                ldrow(O, oldv, rf);
+            else if (i == L - 1)
+                ldrow(O, dbo, x0);
+            // prefetch what the next step needs
+            if (more) {
+                if (nx_down) {
+                    ldrow(Cn, A, sb + (long long)(y + 1) * w + x0);
+                    if (kDim == 3) ldrow(Qn, zin, (long long)(y + 1) * w + x0);
+                } else if (nx_turn) {
+                    if (has_u) ldrow(Cn, gu, x0);
+                } else {
+                    ldrow(Cn, out, sb + (long long)(y - 1) * w + x0);   // its down-sweep result
                 }
-            } else if (nx_turn) {
-#pragma unroll
-                for (int s = 0; s < S; s++) V[s] = has_u ? closer(Pr[s], yshift(Cn[s], cw)) : Pr[s];
+            }
+            // the next step's row before its x passes, from this step's result X
+            auto next_edge = [&](const Cell (&X)[S]) -> Cell {
+                const Cell e = seg_edge<Cell, S, +1>(X, n);
+                if (nx_down) {
+                    const Cell cb = kDim == 3 ? zpull(seg_edge<Cell, S, +1>(Cn, n), seg_edge<Cell, S, +1>(Qn, n))
+                                              : seg_edge<Cell, S, +1>(Cn, n);
+                    return closer(cb, yshift(e, -cw));
+                }
+                if (nx_turn) return has_u ? closer(e, yshift(seg_edge<Cell, S, +1>(Cn, n), cw)) : e;
+                return closer(seg_edge<Cell, S, +1>(Cn, n), yshift(e, cw));
+            };
+            if (pass) {
+                const Cell in0 = (active && t > 0) ? sh.guess[g][t - 1] : V[0];
+                row_pass<Cell, S, false, +1>(Rr, V, t, nseg, n, cw, sh, D, in0, [&](const Cell (&X)[S]) {
+                    if (active) sh.guess[g ^ 1][t] = X[0];
+                });
+                g ^= 1;
+                const Cell in1 = (active && t + 1 < nseg) ? sh.guess[g][t + 1] : Rr[0];
+                row_pass<Cell, S, false, -1>(Pr, Rr, t, nseg, n, cw, sh, D, in1, [&](const Cell (&X)[S]) {
+                    if (more && active) sh.guess[g ^ 1][t] = next_edge(X);
+                });
+                g ^= 1;
             } else {
 #pragma unroll
-                for (int s = 0; s < S; s++) V[s] = closer(Cn[s], yshift(Pr[s], cw));
+                for (int s = 0; s < S; s++) Pr[s] = V[s];
+                if (more && active) sh.guess[g][t] = next_edge(Pr);
+                __syncthreads();
+            }
+            if (down) {
+                strow(out, rf, Pr);
+                if (i == L - 1) {
+#pragma unroll
+                    for (int s = 0; s < S; s++)
+                        if (s < n && !same(O[s], Pr[s])) bits |= kChgDown | kChgAny;
+                    strow(dbn, x0, Pr);
+                }
+            } else {
+                bool diff = false;
+#pragma unroll
+                for (int s = 0; s < S; s++)
+                    if (s < n && !same(O[s], Pr[s])) diff = true;
+                if (diff) bits |= kChgAny | (last ? kChgLast : 0) | (y == y0 ? kChgFirst : 0);
+                strow(out, rf, Pr);
+            }
+            if (more) {
+                if (nx_down) {
+#pragma unroll
+                    for (int s = 0; s < S; s++) {
+                        const Cell cb = kDim == 3 ? zpull(Cn[s], Qn[s]) : Cn[s];
+                        V[s] = closer(cb, yshift(Pr[s], -cw));
+                    }
+                } else if (nx_turn) {
+#pragma unroll
+                    for (int s = 0; s < S; s++) V[s] = has_u ? closer(Pr[s], yshift(Cn[s], cw)) : Pr[s];
+                } else {
+#pragma unroll
+                    for (int s = 0; s < S; s++) V[s] = closer(Cn[s], yshift(Pr[s], cw));
+                }
             }
         }
     }
@@ -295,7 +310,7 @@ __device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cel
 }
 
 template <class Cell, int kDim, int S>
-__global__ void __launch_bounds__(kBlkThreads) k_dan_blocks(DanBlk p)
+__global__ void __launch_bounds__(kBlkThreads, S == 1 ? 3 : 2) k_dan_blocks(DanBlk p)
 {
     __shared__ ScanShared<Cell, kBlkThreads> sh;
     __shared__ int s_item, s_chg;
@@ -325,13 +340,13 @@ __global__ void __launch_bounds__(kBlkThreads) k_dan_blocks(DanBlk p)
                 const int bits = s_chg;
                 p.chg[b] = (uint8_t)bits;
                 if (bits) {
-                    const int z = kDim == 3 ? b / p.nc : 0;
-                    const int c = b - z * p.nc;
+                    const int k = b / p.nc;
+                    const int c = b - k * p.nc;
                     auto queue = [&](int dep) {
                         if (atomicMax(p.stamp + dep, round + 1) < round + 1)
                             wln[atomicAdd(p.ctl + (cur ^ 1), 1u)] = dep;
                     };
-                    if ((bits & kChgRows) && kDim == 3 && z + p.dir >= 0 && z + p.dir < p.d) queue(b + p.dir * p.nc);
+                    if ((bits & kChgLast) && k + 1 < p.nk) queue(b + p.nc);
                     if ((bits & kChgFirst) && c > 0) queue(b - 1);
                     if ((bits & kChgDown) && c + 1 < p.nc) queue(b + 1);
                 }
@@ -342,7 +357,7 @@ __global__ void __launch_bounds__(kBlkThreads) k_dan_blocks(DanBlk p)
         // commit: blocks whose output changed now hold it in the other version
         for (unsigned i = blockIdx.x * blockDim.x + t; i < nwork; i += gridDim.x * blockDim.x) {
             const int b = __ldcg(wl + i);
-            if (__ldcg(p.chg + b)) p.lat[b] = __ldcg(p.lat + b) == 0 ? 1 : 0;
+            if (__ldcg(p.chg + b) & kChgAny) p.lat[b] = __ldcg(p.lat + b) == 0 ? 1 : 0;
         }
         if (blockIdx.x == 0 && t == 0) {
             p.ctl[2] = 0;
@@ -354,24 +369,17 @@ __global__ void __launch_bounds__(kBlkThreads) k_dan_blocks(DanBlk p)
     if (blockIdx.x == 0 && t == 0) p.ctl[5] = (unsigned)(round + 1);
 }
 
-// every block takes its rows from the input; all blocks but the fixed slice's are queued
+// every block takes its rows from the input, and all are queued
 __global__ void k_dan_blocks_init(DanBlk p)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < p.nblocks; b += gridDim.x * blockDim.x) {
         p.lat[b] = 2;
         p.chg[b] = 0;
         p.stamp[b] = 0;
-        const int z = b / p.nc;
-        if (p.zfix < 0) {
-            p.wl[0][b] = b;
-        } else if (z != p.zfix) {
-            // fixed slice first (forward: slice 0) or last (backward: slice d-1)
-            const int k = p.zfix == 0 ? b - p.nc : b;
-            p.wl[0][k] = b;
-        }
+        p.wl[0][b] = b;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        p.ctl[0] = (unsigned)(p.zfix < 0 ? p.nblocks : p.nblocks - p.nc);
+        p.ctl[0] = (unsigned)p.nblocks;
         for (int i = 1; i < 8; i++) p.ctl[i] = 0;
     }
 }
@@ -387,7 +395,9 @@ __global__ void k_dan_blocks_store(DanBlk p, typename CellIO<Cell>::P* __restric
          i += (long long)gridDim.x * blockDim.x) {
         const int z = (int)(i / plane);
         const int y = (int)((i - z * plane) / p.w);
-        const int v = p.lat[z * p.nc + y / p.R];
+        const int pos = (z - p.zfirst) * p.dir;
+        if (pos < 0 || pos >= p.nchain) continue;   // the fixed slice
+        const int v = p.lat[(pos / p.Z) * p.nc + y / p.R];
         if (v != 2) {
             const P* src = static_cast<const P*>(p.V[v]);
 #pragma unroll
@@ -420,16 +430,27 @@ size_t dan_blocks_workspace_bytes(int dim, int w, int h, int d, int R)
 template <class Cell, int kDim, int S>
 static bool run_phase(DanBlk& p, void* dl, cudaStream_t st)
 {
-    k_dan_blocks_init<<<(p.nblocks + 255) / 256, 256, 0, st>>>(p);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dan_blocks<Cell, kDim, S>, kBlkThreads, 0) !=
             cudaSuccess ||
         per_sm < 1)
         return false;
-    int grid = per_sm * g_num_sms;
-    const int work = p.zfix < 0 ? p.nblocks : p.nblocks - p.nc;
-    if (grid > work) grid = work;
-    if (grid < 1) grid = 1;
+    const int resident = per_sm * g_num_sms;
+    // slices per block: long enough that few rounds are needed, short enough
+    // that about four block columns per resident CTA keep every SM busy
+    int Z = tune_get(kTuneDanSlices, p.w);
+    if (Z < 1) {
+        const long long cols = 4LL * resident;
+        Z = (int)((long long)p.nchain * p.nc / cols);
+        if (Z < 1) Z = 1;
+    }
+    if (Z > p.nchain) Z = p.nchain;
+    p.Z = Z;
+    p.nk = (p.nchain + Z - 1) / Z;
+    p.nblocks = p.nk * p.nc;
+    p.max_rounds = 2 * p.nblocks + 8;
+    k_dan_blocks_init<<<(p.nblocks + 255) / 256, 256, 0, st>>>(p);
+    int grid = resident < p.nblocks ? resident : p.nblocks;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kBlkThreads);
@@ -453,7 +474,7 @@ static bool run_all(int w, int h, int d, int cw, int R, void* deltas, void* ws, 
     const size_t cb = kDim == 3 ? 6 : 4;
     const size_t cells = (size_t)w * h * d;
     const int nc = (h + R - 1) / R;
-    const int nb = nc * d;
+    const int nb = nc * d;   // (slice, chunk) pairs: down-boundary row slots, and a bound on the blocks
     char* q = static_cast<char*>(ws);
     DanBlk p{};
     p.A = deltas;
@@ -483,18 +504,19 @@ static bool run_all(int w, int h, int d, int cw, int R, void* deltas, void* ws, 
     p.R = R;
     p.nc = nc;
     p.cw = cw;
-    p.nblocks = nb;
-    p.max_rounds = 2 * nb + 8;
     if (kDim == 2) {
         p.dir = 1;
-        p.zfix = -1;
+        p.zfirst = 0;
+        p.nchain = 1;
         return run_phase<Cell, kDim, S>(p, deltas, st);
     }
+    // slices 1..d-1 pull from the slice before, then d-2..0 from the slice after
     p.dir = 1;
-    p.zfix = 0;
+    p.zfirst = 1;
+    p.nchain = d - 1;
     if (!run_phase<Cell, kDim, S>(p, deltas, st)) return false;
     p.dir = -1;
-    p.zfix = d - 1;
+    p.zfirst = d - 2;
     return run_phase<Cell, kDim, S>(p, deltas, st);
 }
 

@@ -845,11 +845,11 @@ __device__ __noinline__ void batch_item_warp(const BatchItemDev& b, const uint32
     }
 }
 
-// Items are ordered with the wide ones (rows > 256 cells: whole-CTA engine)
-// first, largest work first, then the narrow ones.  A CTA draws items one at a
-// time while they are wide; the first narrow item it draws switches it to
-// per-warp draining: each warp takes narrow items on its own until the queue
-// is empty.
+// Items are ordered volumes first (their serial chains are the longest), then
+// wide images (rows > 256 cells), each by decreasing work, then the narrow
+// images: all of these but the narrow images take a whole CTA each.  The first
+// narrow image a CTA draws switches it to per-warp draining: each warp takes
+// narrow images on its own until the queue is empty.
 template <int S>
 __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restrict__ items, const int* __restrict__ order,
                                                    int n, const uint32_t* __restrict__ masks,
@@ -867,8 +867,8 @@ __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restric
         __syncthreads();
         if (it >= n) return;
         const BatchItemDev b = items[order[it]];
-        if (b.w <= 256) {
-            // narrow from here on: warp 0 takes this item, every warp then drains the queue
+        if (b.d <= 1 && b.w <= 256) {
+            // narrow images from here on: warp 0 takes this item, every warp then drains the queue
             int mine = warp == 0 ? it : -1;
             for (;;) {
                 if (mine < 0) {

@@ -36,6 +36,7 @@ enum TuneKind {
     kTuneBatch,
     kTuneEdt,
     kTuneDanRows,
+    kTuneDanSlices,
     kTuneKinds
 };
 int tune_get(int kind, int w);

@@ -81,6 +81,7 @@ static std::vector<int> candidates(int kind, int w)
         case kTuneBatch: return {4, 8};
         case kTuneEdt: return {256, 512};
         case kTuneDanRows: return {4, 8, 16, 32, kDanSerial};
+        case kTuneDanSlices: return {1, 4, 16, 64};
     }
     return {};
 }
@@ -155,7 +156,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (kind == kTuneBatch) return tune_batch(st);
     const bool vol = kind == kTuneDan3 || kind == kTuneFs3 || kind == kTuneJfa3 || kind == kTuneEdt ||
-                     (kind == kTuneDanRows && d > 1);
+                     ((kind == kTuneDanRows && d > 1) || kind == kTuneDanSlices);
     // a bounded synthetic problem of the caller's row / line shape
     int tw = w, th = h, td = vol ? d : 1;
     if (kind == kTuneDan2 || kind == kTuneFs2) th = h < 256 ? h : 256;
@@ -164,7 +165,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
         td = d < 8 ? d : 8;
     }
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);
-    if (kind == kTuneJfa3 || kind == kTuneEdt || kind == kTuneDanRows) {
+    if (kind == kTuneJfa3 || kind == kTuneEdt || kind == kTuneDanRows || kind == kTuneDanSlices) {
         while ((long long)tw * th * td > (1LL << 26) && td > 1) td = (td + 1) / 2;
     }
     const long long cells = (long long)tw * th * td;
@@ -186,7 +187,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     void *dm = nullptr, *dl = nullptr, *tmp = nullptr, *ws = nullptr;
     const size_t cell_bytes = vol ? 6 : 4;
     size_t ws_bytes = kind == kTuneEdt       ? edt_workspace_bytes(3, tw, th, td)
-                      : kind == kTuneDanRows ? dan_blocks_workspace_bytes(vol ? 3 : 2, tw, th, td, 1)
+                      : (kind == kTuneDanRows || kind == kTuneDanSlices) ? dan_blocks_workspace_bytes(vol ? 3 : 2, tw, th, td, 1)
                                              : fastsweep3_workspace_bytes(tw, th, td);
     bool ok = cudaMallocAsync(&dm, mwords * 4, st) == cudaSuccess &&
               cudaMallocAsync(&dl, (size_t)cells * (kind == kTuneEdt ? 4 : cell_bytes), st) == cudaSuccess &&
@@ -231,6 +232,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
                                 err, st);
                 break;
             case kTuneDanRows:
+            case kTuneDanSlices:
                 launch_init_border(dim, static_cast<uint32_t*>(dm), dl, tw, th, td, st);
                 run_danielsson(dim, dl, tw, th, td, 2, ws, ws_bytes, err, st);
                 break;

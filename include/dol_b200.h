@@ -252,6 +252,7 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_EDT           7   /* threads per CTA of the line passes: 256 or 512 */
 #define DOL_TUNE_DANIELSSON_ROWS 8 /* Danielsson block schedule: rows per block (1..4096);
                                       65536 = the serial single-CTA engine */
+#define DOL_TUNE_DANIELSSON_SLICES 9 /* Danielsson block schedule: slices per block (3D) */
 DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream);
 DOL_API int        dol_tune_get(int kind, int w);
 DOL_API void       dol_tune_set(int kind, int w, int value);

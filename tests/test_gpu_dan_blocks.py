@@ -1,13 +1,13 @@
 """Danielsson's block schedule (fixed-point iteration over blocks of rows)
 against the oracle's serial Danielsson, bit for bit, for every rows-per-block
-value and cells-per-thread engine, on masks of awkward shapes and densities,
+value, slices-per-block value and cells-per-thread engine, on masks of awkward shapes and densities,
 signed (border init, cw = 2) and unsigned (cw = 1)."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-TUNE_DAN2, TUNE_DAN3, TUNE_ROWS = 0, 1, 8
+TUNE_DAN2, TUNE_DAN3, TUNE_ROWS, TUNE_SLICES = 0, 1, 8, 9
 SERIAL = 65536
 
 
@@ -59,11 +59,13 @@ SHAPES3 = [(37, 29, 23), (64, 17, 40), (5, 80, 9), (130, 33, 12), (1, 20, 30), (
 SHAPES2 = [(200, 150), (1024, 77), (33, 500), (1, 300), (300, 1), (517, 260)]
 
 
+@pytest.mark.parametrize("slices", [1, 2, 5, 1000])
 @pytest.mark.parametrize("rows", [1, 3, 8, 64])
 @pytest.mark.parametrize("dims", SHAPES3)
-def test_blocks_3d(dol, O, cuda, tune, dims, rows):
-    rng = np.random.default_rng(sum(dims) + rows)
+def test_blocks_3d(dol, O, cuda, tune, dims, rows, slices):
+    rng = np.random.default_rng(sum(dims) + rows + slices)
     tune(TUNE_ROWS, dims[0], rows)
+    tune(TUNE_SLICES, dims[0], slices)
     for i, m in enumerate([rand_mask(O, rng, dims, 0.002), rand_mask(O, rng, dims, 0.3), blob_mask(O, rng, dims, 3),
                            rand_mask(O, rng, dims, 0.0)]):
         for cw, signed in ((2, True), (1, False)):

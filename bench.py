@@ -268,7 +268,7 @@ def _sweep_variants(dol, torch, res, L, sp, big=True):
     work3 = base3.clone()
     for rows in (4, 8, 16, 32):
         L.dol_tune_set(ROWS, n, rows)
-        for z in (1, 2, 4, 8, 16, 32, 64, 0):
+        for z in (2, 4, 8, 16, 0):
             L.dol_tune_set(SLICES, n, z)
             out[f"3d_256_rows{rows}_slices{z or 'auto'}_ms"] = timed(work3, base3, dims3, 2)
     L.dol_tune_set(ROWS, n, 0)
@@ -283,14 +283,17 @@ def _sweep_variants(dol, torch, res, L, sp, big=True):
         mdv = torch.empty(dol.mask_words(side, side, side), dtype=torch.int32, device="cuda")
         dol.check(L.dol_gen_value_noise_3d(side, side, side, SPACING, C.c_uint32(SEED), C.c_void_p(mdv.data_ptr()), sp))
         dv = torch.empty((side, side, side, 3), dtype=torch.int16, device="cuda")
-        for rows, z in ((8, 0), (8, 32), (8, 64), (8, 128), (8, 256), (16, 0), (4, 0)):
+        for rows, z, s_ in ((8, 0, 0), (8, 32, 0), (8, 64, 0), (16, 32, 0), (8, 32, 2), (8, 32, 8), (16, 32, 8)):
             L.dol_tune_set(ROWS, side, rows)
             L.dol_tune_set(SLICES, side, z)
+            L.dol_tune_set(DAN3, side, s_)
             dol.init_border(mdv, (side,) * 3, out=dv)
             torch.cuda.synchronize()
-            out[f"3d_1024_rows{rows}_slices{z or 'auto'}_ms"] = _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)
+            out[f"3d_1024_rows{rows}_slices{z or 'auto'}_s{s_ or 'auto'}_ms"] = \
+                _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)
         L.dol_tune_set(ROWS, side, 0)
         L.dol_tune_set(SLICES, side, 0)
+        L.dol_tune_set(DAN3, side, 0)
         del dv, mdv
     res["danielsson_variants"] = out
 
@@ -594,6 +597,27 @@ def run_dol(args):
         pg.destroy_process_group()
 
 
+def danielsson_only(shape):
+    """Signed Danielsson (border init, cw = 2) on a value-noise volume of the
+    given shape, run twice with CUDA events around each run."""
+    import torch
+    dol = load_dol()
+    L = dol.lib()
+    w, h, d = (int(v) for v in shape.split("x"))
+    dims = (w, h, d)
+    md = torch.empty(dol.mask_words(*dims), dtype=torch.int32, device="cuda")
+    dol.check(L.dol_gen_value_noise_3d(w, h, d, SPACING, C.c_uint32(SEED), C.c_void_p(md.data_ptr()), None))
+    base = dol.init_border(md, dims)
+    work = base.clone()
+    times = []
+    for _ in range(2):
+        work.copy_(base)
+        torch.cuda.synchronize()
+        times.append(_ev_ms(torch, lambda: dol.danielsson(work, dims, 2), 1))
+    dol.sync()
+    print(json.dumps({"danielsson_signed": shape, "ms": times}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -610,12 +634,16 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration measurements")
     ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
     ap.add_argument("--only", default=None,
-                    help="comma list of c1,c2,c3,c4: run only these per-configuration measurements (no headline)")
+                    help="comma list of c1..c6: run only these per-configuration measurements (no headline)")
+    ap.add_argument("--danielsson", default=None, metavar="WxHxD",
+                    help="only time signed Danielsson on a WxHxD value-noise volume (twice; for profiling)")
     args = ap.parse_args()
     global W, H, D
     W = H = D = args.side
     if args.impl == "reference":
         run_reference(args)
+    elif args.danielsson:
+        danielsson_only(args.danielsson)
     elif args.only:
         import torch
         dol = load_dol()

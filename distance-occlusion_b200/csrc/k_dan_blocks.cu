@@ -34,7 +34,7 @@
 
 namespace dolk {
 
-constexpr int kBlkThreads = 256;
+constexpr int kBlkThreads = 256;   // the widest CTA (rows up to 8 x 256 cells)
 
 template <class Cell>
 struct CellIO;
@@ -131,8 +131,8 @@ constexpr int kChgAny = 8;     // any output changed: the block's version flips
 
 // One block: rows y0..y1-1 of Z consecutive slices (in the phase's order),
 // T threads of S cells each.
-template <class Cell, int kDim, int S>
-__device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cell, kBlkThreads>& sh, int* s_chg)
+template <class Cell, int kDim, int S, int T>
+__device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cell, T>& sh, int* s_chg)
 {
     using IO = CellIO<Cell>;
     using P = typename IO::P;
@@ -309,10 +309,12 @@ __device__ __forceinline__ void dan_block(const DanBlk& p, int b, ScanShared<Cel
     __syncthreads();
 }
 
-template <class Cell, int kDim, int S>
-__global__ void __launch_bounds__(kBlkThreads, S == 1 ? 3 : 2) k_dan_blocks(DanBlk p)
+// T threads per CTA (a multiple of 32 covering the row's segments); the
+// register budget allows 512 / T * ... CTAs: 128 registers a thread
+template <class Cell, int kDim, int S, int T>
+__global__ void __launch_bounds__(T, 512 / T) k_dan_blocks(DanBlk p)
 {
-    __shared__ ScanShared<Cell, kBlkThreads> sh;
+    __shared__ ScanShared<Cell, T> sh;
     __shared__ int s_item, s_chg;
     const int t = threadIdx.x;
     const unsigned long long kLimit = 20ull * 1000 * 1000 * 1000;   // 20 s per barrier wait
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(kBlkThreads, S == 1 ? 3 : 2) k_dan_blocks(DanB
             const unsigned it = (unsigned)s_item;
             if (it >= nwork) break;
             const int b = __ldcg(wl + it);
-            dan_block<Cell, kDim, S>(p, b, sh, &s_chg);   // ends with a barrier
+            dan_block<Cell, kDim, S, T>(p, b, sh, &s_chg);   // ends with a barrier
             if (t == 0) {
                 const int bits = s_chg;
                 p.chg[b] = (uint8_t)bits;
@@ -427,11 +429,11 @@ size_t dan_blocks_workspace_bytes(int dim, int w, int h, int d, int R)
     return 2 * al256(cells * cb) + 2 * al256(nb * w * cb) + 2 * al256(nb) + 3 * al256(nb * sizeof(int)) + 256;
 }
 
-template <class Cell, int kDim, int S>
+template <class Cell, int kDim, int S, int T>
 static bool run_phase(DanBlk& p, void* dl, cudaStream_t st)
 {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dan_blocks<Cell, kDim, S>, kBlkThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dan_blocks<Cell, kDim, S, T>, T, 0) !=
             cudaSuccess ||
         per_sm < 1)
         return false;
@@ -453,14 +455,14 @@ static bool run_phase(DanBlk& p, void* dl, cudaStream_t st)
     int grid = resident < p.nblocks ? resident : p.nblocks;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kBlkThreads);
+    cfg.blockDim = dim3(T);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_dan_blocks<Cell, kDim, S>, p) != cudaSuccess) return false;
+    if (cudaLaunchKernelEx(&cfg, k_dan_blocks<Cell, kDim, S, T>, p) != cudaSuccess) return false;
     const long long cells = (long long)p.w * p.h * p.d;
     long long gb = (cells + 255) / 256;
     if (gb > (long long)g_num_sms * 32) gb = (long long)g_num_sms * 32;
@@ -468,7 +470,7 @@ static bool run_phase(DanBlk& p, void* dl, cudaStream_t st)
     return true;
 }
 
-template <class Cell, int kDim, int S>
+template <class Cell, int kDim, int S, int T>
 static bool run_all(int w, int h, int d, int cw, int R, void* deltas, void* ws, int* err, cudaStream_t st)
 {
     const size_t cb = kDim == 3 ? 6 : 4;
@@ -508,16 +510,16 @@ static bool run_all(int w, int h, int d, int cw, int R, void* deltas, void* ws, 
         p.dir = 1;
         p.zfirst = 0;
         p.nchain = 1;
-        return run_phase<Cell, kDim, S>(p, deltas, st);
+        return run_phase<Cell, kDim, S, T>(p, deltas, st);
     }
     // slices 1..d-1 pull from the slice before, then d-2..0 from the slice after
     p.dir = 1;
     p.zfirst = 1;
     p.nchain = d - 1;
-    if (!run_phase<Cell, kDim, S>(p, deltas, st)) return false;
+    if (!run_phase<Cell, kDim, S, T>(p, deltas, st)) return false;
     p.dir = -1;
     p.zfirst = d - 2;
-    return run_phase<Cell, kDim, S>(p, deltas, st);
+    return run_phase<Cell, kDim, S, T>(p, deltas, st);
 }
 
 size_t danielsson_workspace_bytes(int dim, int w, int h, int d)
@@ -542,15 +544,26 @@ bool launch_danielsson_blocks(int dim, void* deltas, int w, int h, int d, int cw
 {
     if (dim == 3 && d < 2) return true;   // the reference's slice loops do not run
     ProfScope ps("danielsson_blocks", st);
+    // cells per thread: tuned, else the fewest that keep the row within 128
+    // threads (short segments, CTAs of 2-4 warps); 3D cells stop at 4 per
+    // thread, where the register file still holds every array
     int s = tune_get(dim == 2 ? kTuneDan2 : kTuneDan3, w);
-    if (s != 1 && s != 2 && s != 4 && s != 8) s = 0;
-    if (!s) s = w <= 256 ? 1 : (w <= 512 ? 2 : (w <= 1024 ? 4 : 8));
+    if (s != 1 && s != 2 && s != 4 && s != 8) {
+        s = 1;
+        while ((w + s - 1) / s > 128 && s < (dim == 3 ? 4 : 8)) s *= 2;
+    }
     while ((w + s - 1) / s > kBlkThreads && s < 8) s *= 2;
-    if ((w + s - 1) / s > kBlkThreads) return false;
+    const int nseg = (w + s - 1) / s;
+    if (nseg > kBlkThreads) return false;
+    const int t = nseg <= 64 ? 64 : (nseg <= 128 ? 128 : 256);
+#define DOL_BLK_RUN(SV, TV)                                                                             \
+    return dim == 2 ? run_all<C2, 2, SV, TV>(w, h, 1, cw, R, deltas, ws, err, st)                     \
+                    : run_all<C3, 3, SV, TV>(w, h, d, cw, R, deltas, ws, err, st);
 #define DOL_BLK_CASE(SV)                                                                                \
     case SV:                                                                                            \
-        return dim == 2 ? run_all<C2, 2, SV>(w, h, 1, cw, R, deltas, ws, err, st)                      \
-                        : run_all<C3, 3, SV>(w, h, d, cw, R, deltas, ws, err, st);
+        if (t == 64) { DOL_BLK_RUN(SV, 64) }                                                            \
+        if (t == 128) { DOL_BLK_RUN(SV, 128) }                                                          \
+        DOL_BLK_RUN(SV, 256)
     switch (s) {
         DOL_BLK_CASE(1)
         DOL_BLK_CASE(2)
@@ -559,6 +572,7 @@ bool launch_danielsson_blocks(int dim, void* deltas, int w, int h, int d, int cw
         default: break;
     }
 #undef DOL_BLK_CASE
+#undef DOL_BLK_RUN
     return false;
 }
 

@@ -241,11 +241,17 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
 // s and 0 otherwise, so for a cell of state s every probe is one load, one
 // multiply-add (or add) and one min -- a cell of the other state at distance k
 // contributes exactly k^2.  The symmetric part of the walk runs without bounds
-// checks; lanes cover TX columns x (32/TX) adjacent positions.
+// checks; a warp covers 8 columns x 4 adjacent positions.
 template <typename TIn>
 __device__ __forceinline__ uint32_t sq_val(TIn v)
 {
     return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v : (uint32_t)v;
+}
+// sq_val(v) + k2: one multiply-add for the u16 (distance) form
+template <typename TIn>
+__device__ __forceinline__ uint32_t add_sq(TIn v, uint32_t k2)
+{
+    return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v + k2 : (uint32_t)v + k2;
 }
 
 template <typename TIn, bool kFinal, int TX>
@@ -290,41 +296,54 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     }
     __syncthreads();
 
-    constexpr int kRowsPerWarp = 32 / TX;
-    const int lane = threadIdx.x & 31, col = lane % TX, sub = lane / TX;
-    const int nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
+    // a warp covers 8 columns x 4 positions (a compact footprint: neighbouring
+    // cells have similar search lengths, and the 32 probes of a step fall in
+    // distinct shared-memory banks); TX / 8 column groups per CTA
+    constexpr int kGroups = TX / 8;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
+    const int col = (wi % kGroups) * 8 + (lane & 7), sub = lane >> 3;
+    const int qstep = 4 * (nw / kGroups);
     const int x = x0 + col;
     if (x >= w) return;
     const long long base = (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-    for (int q = kRowsPerWarp * wi + sub; q < n; q += kRowsPerWarp * nw) {
+    for (int q = 4 * (wi / kGroups) + sub; q < n; q += qstep) {
         const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
         const TIn* A = (s ? F1 : F0) + col;
         uint32_t best = sq_val<TIn>(A[q * TX]);
         const int lmax = q, rmax = n - 1 - q, kmin = min(lmax, rmax);
-        uint32_t k2 = 1, dk = 3;
         int k = 1;
+        uint32_t k2 = 1;   // k^2
         const TIn* pl = A + (q - 1) * TX;
         const TIn* pr = A + (q + 1) * TX;
-        for (; k <= kmin && k2 < best; k++) {
-            best = min(best, min(sq_val<TIn>(*pl), sq_val<TIn>(*pr)) + k2);
+        // both sides, two distances per trip (at most one probe past the stop,
+        // which cannot lower the minimum below its exact value)
+        for (; k + 1 <= kmin && k2 < best; k += 2) {
+            const uint32_t k2b = k2 + 2 * k + 1;   // (k+1)^2
+            best = min(best, min(add_sq<TIn>(pl[0], k2), add_sq<TIn>(pr[0], k2)));
+            best = min(best, min(add_sq<TIn>(pl[-TX], k2b), add_sq<TIn>(pr[TX], k2b)));
+            pl -= 2 * TX;
+            pr += 2 * TX;
+            k2 = k2b + 2 * k + 3;   // (k+2)^2
+        }
+        if (k <= kmin && k2 < best) {
+            best = min(best, min(add_sq<TIn>(pl[0], k2), add_sq<TIn>(pr[0], k2)));
             pl -= TX;
             pr += TX;
-            k2 += dk;
-            dk += 2;
+            k2 += 2 * k + 1;
+            k++;
         }
+        // one side left
         for (; k <= lmax && k2 < best; k++) {
-            best = min(best, sq_val<TIn>(*pl) + k2);
+            best = min(best, add_sq<TIn>(*pl, k2));
             pl -= TX;
-            k2 += dk;
-            dk += 2;
+            k2 += 2 * k + 1;
         }
         for (; k <= rmax && k2 < best; k++) {
-            best = min(best, sq_val<TIn>(*pr) + k2);
+            best = min(best, add_sq<TIn>(*pr, k2));
             pr += TX;
-            k2 += dk;
-            dk += 2;
+            k2 += 2 * k + 1;
         }
         put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }

@@ -159,11 +159,12 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
                      ((kind == kTuneDanRows && d > 1) || kind == kTuneDanSlices);
     // a bounded synthetic problem of the caller's row / line shape
     int tw = w, th = h, td = vol ? d : 1;
-    if (kind == kTuneDan2 || kind == kTuneFs2) th = h < 256 ? h : 256;
-    if (kind == kTuneDan3 || kind == kTuneFs3) {
+    if (kind == kTuneFs2) th = h < 256 ? h : 256;
+    if (kind == kTuneFs3) {
         th = h < 64 ? h : 64;
         td = d < 8 ? d : 8;
     }
+    if (kind == kTuneDan3) td = d < 32 ? d : 32;   // whole slices: the block schedule's row blocks
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);
     if (kind == kTuneJfa3 || kind == kTuneEdt || kind == kTuneDanRows || kind == kTuneDanSlices) {
         while ((long long)tw * th * td > (1LL << 26) && td > 1) td = (td + 1) / 2;
@@ -186,9 +187,10 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     }
     void *dm = nullptr, *dl = nullptr, *tmp = nullptr, *ws = nullptr;
     const size_t cell_bytes = vol ? 6 : 4;
-    size_t ws_bytes = kind == kTuneEdt       ? edt_workspace_bytes(3, tw, th, td)
-                      : (kind == kTuneDanRows || kind == kTuneDanSlices) ? dan_blocks_workspace_bytes(vol ? 3 : 2, tw, th, td, 1)
-                                             : fastsweep3_workspace_bytes(tw, th, td);
+    const bool dan = kind == kTuneDan2 || kind == kTuneDan3 || kind == kTuneDanRows || kind == kTuneDanSlices;
+    size_t ws_bytes = kind == kTuneEdt ? edt_workspace_bytes(3, tw, th, td)
+                      : dan            ? dan_blocks_workspace_bytes(vol ? 3 : 2, tw, th, td, 1)
+                                       : fastsweep3_workspace_bytes(tw, th, td);
     bool ok = cudaMallocAsync(&dm, mwords * 4, st) == cudaSuccess &&
               cudaMallocAsync(&dl, (size_t)cells * (kind == kTuneEdt ? 4 : cell_bytes), st) == cudaSuccess &&
               cudaMallocAsync(&tmp, (size_t)cells * cell_bytes, st) == cudaSuccess &&
@@ -210,9 +212,9 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
         const int dim = vol ? 3 : 2;
         switch (kind) {
             case kTuneDan2:
-            case kTuneDan3:
+            case kTuneDan3:   // through the entry path: block schedule or serial engine
                 launch_init_border(dim, static_cast<uint32_t*>(dm), dl, tw, th, td, st);
-                launch_danielsson(dim, dl, tw, th, td, 2, st);
+                run_danielsson(dim, dl, tw, th, td, 2, ws, ws_bytes, err, st);
                 break;
             case kTuneFs2:
                 launch_init_border(2, static_cast<uint32_t*>(dm), dl, tw, th, 1, st);

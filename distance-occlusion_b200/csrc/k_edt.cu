@@ -41,98 +41,132 @@ constexpr uint32_t kInf32 = 0x7FFFFFFFu;    // "no opposite cell in this plane"
 constexpr int kMaxChunks = 32;              // rows up to 32*32*32 = 32768 cells
 
 // ---------------------------------------------------------------- x pass ----
-// One warp per row.  Per word: positions of its last / first clear and set
-// live bits; an exclusive prefix max (left) and suffix min (right) over the
-// words give the nearest cell of either state outside the word.
+// A row is split over the lanes of a warp segment, one mask word (32 cells) per
+// lane: rows of up to 16 words share a warp (segments of 1..16 lanes), longer
+// rows take the whole warp and loop over 32-word chunks.  Segment scans give
+// each word the nearest clear / set cell before and after it (longer rows: a
+// right-to-left pre-pass over the chunks gives the carries from the right).
+// Inside the word a lane walks its 32 cells twice: forwards, the nearest
+// cell of the other state on the left is the cell before the current run
+// (runs change where m ^ (m << 1) has a bit), backwards the cell after it.
+// The 32 results go out as four 16-byte stores.
+__device__ __forceinline__ int pow2_at_least(int v)
+{
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
 __global__ void __launch_bounds__(256) k_edt_x(const uint32_t* __restrict__ mask, uint16_t* __restrict__ out, int w,
                                                long long rows)
 {
     __shared__ int right_carry[8][kMaxChunks][2];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int ws = words_per_row(w);
+    const int SW = ws >= 32 ? 32 : pow2_at_least(ws);   // lanes per row
+    const int seg = lane / SW, sl = lane % SW, rpw = 32 / SW;
     const int nchunks = (ws + 31) >> 5;
     const int NEG = -(1 << 30), POS = 1 << 30;
+    const bool vec_ok = (w & 7) == 0;   // 16-byte aligned word outputs
     long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
 
-    for (long long row = warp; row < rows; row += nwarps) {
-        const uint32_t* mrow = mask + row * ws;
-        uint16_t* orow = out + row * (long long)w;
+    for (long long row0 = warp * rpw; row0 < rows; row0 += nwarps * rpw) {
+        const long long row = row0 + seg;
+        const bool rowok = row < rows;
+        const uint32_t* mrow = mask + (rowok ? row : 0) * ws;
+        uint16_t* orow = out + (rowok ? row : 0) * (long long)w;
 
-        // right-to-left over chunks: first clear / set position right of each chunk
-        int carry0 = POS, carry1 = POS;
-        for (int c = nchunks - 1; c >= 0; c--) {
-            right_carry[wib][c][0] = carry0;
-            right_carry[wib][c][1] = carry1;
-            if (c == 0) break;
-            int k = 32 * c + lane;
-            int f0 = POS, f1 = POS;
-            if (k < ws) {
-                uint32_t live = live_bits(w, k), m = mrow[k];
-                uint32_t z0 = ~m & live, z1 = m & live;
-                if (z0) f0 = 32 * k + __ffs(z0) - 1;
-                if (z1) f1 = 32 * k + __ffs(z1) - 1;
+        // long rows: first clear / set cell right of each chunk (segments are whole warps here)
+        if (nchunks > 1) {
+            int carry0 = POS, carry1 = POS;
+            for (int c = nchunks - 1; c >= 0; c--) {
+                right_carry[wib][c][0] = carry0;
+                right_carry[wib][c][1] = carry1;
+                if (c == 0) break;
+                const int k = 32 * c + lane;
+                int f0 = POS, f1 = POS;
+                if (k < ws) {
+                    const uint32_t live = live_bits(w, k), m = mrow[k];
+                    const uint32_t z0 = ~m & live, z1 = m & live;
+                    if (z0) f0 = 32 * k + __ffs(z0) - 1;
+                    if (z1) f1 = 32 * k + __ffs(z1) - 1;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    f0 = min(f0, __shfl_xor_sync(0xFFFFFFFFu, f0, o));
+                    f1 = min(f1, __shfl_xor_sync(0xFFFFFFFFu, f1, o));
+                }
+                carry0 = min(carry0, f0);
+                carry1 = min(carry1, f1);
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                f0 = min(f0, __shfl_xor_sync(0xFFFFFFFFu, f0, o));
-                f1 = min(f1, __shfl_xor_sync(0xFFFFFFFFu, f1, o));
-            }
-            carry0 = min(carry0, f0);
-            carry1 = min(carry1, f1);
+            __syncwarp();
         }
-        __syncwarp();
 
-        int left0 = NEG, left1 = NEG;   // last clear / set position left of the chunk
+        int left0 = NEG, left1 = NEG;   // last clear / set cell left of the chunk
         for (int c = 0; c < nchunks; c++) {
-            int k = 32 * c + lane;
+            const int k = 32 * c + sl;
+            const bool on = rowok && sl < SW && k < ws && (nchunks > 1 || sl < ws);
             uint32_t m = 0, live = 0;
             int l0 = NEG, l1 = NEG, f0 = POS, f1 = POS;
-            if (k < ws) {
+            if (on) {
                 m = mrow[k];
                 live = live_bits(w, k);
-                uint32_t z0 = ~m & live, z1 = m & live;
+                const uint32_t z0 = ~m & live, z1 = m & live;
                 if (z0) { l0 = 32 * k + 31 - __clz(z0); f0 = 32 * k + __ffs(z0) - 1; }
                 if (z1) { l1 = 32 * k + 31 - __clz(z1); f1 = 32 * k + __ffs(z1) - 1; }
             }
-            // exclusive prefix max of last positions, exclusive suffix min of first positions
+            // segment-exclusive prefix max of last positions, suffix min of first positions
             int p0 = l0, p1 = l1, s0 = f0, s1 = f1;
-            for (int o = 1; o < 32; o <<= 1) {
-                int a0 = __shfl_up_sync(0xFFFFFFFFu, p0, o), a1 = __shfl_up_sync(0xFFFFFFFFu, p1, o);
-                int b0 = __shfl_down_sync(0xFFFFFFFFu, s0, o), b1 = __shfl_down_sync(0xFFFFFFFFu, s1, o);
-                if (lane >= o) { p0 = max(p0, a0); p1 = max(p1, a1); }
-                if (lane + o < 32) { s0 = min(s0, b0); s1 = min(s1, b1); }
+            for (int o = 1; o < SW; o <<= 1) {
+                const int a0 = __shfl_up_sync(0xFFFFFFFFu, p0, o, SW), a1 = __shfl_up_sync(0xFFFFFFFFu, p1, o, SW);
+                const int b0 = __shfl_down_sync(0xFFFFFFFFu, s0, o, SW), b1 = __shfl_down_sync(0xFFFFFFFFu, s1, o, SW);
+                if (sl >= o) { p0 = max(p0, a0); p1 = max(p1, a1); }
+                if (sl + o < SW) { s0 = min(s0, b0); s1 = min(s1, b1); }
             }
-            int ex0 = __shfl_up_sync(0xFFFFFFFFu, p0, 1), ex1 = __shfl_up_sync(0xFFFFFFFFu, p1, 1);
-            int ey0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1), ey1 = __shfl_down_sync(0xFFFFFFFFu, s1, 1);
-            if (lane == 0) { ex0 = NEG; ex1 = NEG; }
-            if (lane == 31) { ey0 = POS; ey1 = POS; }
-            ex0 = max(ex0, left0); ex1 = max(ex1, left1);
-            ey0 = min(ey0, right_carry[wib][c][0]); ey1 = min(ey1, right_carry[wib][c][1]);
-            // chunk totals feed the next chunk
-            int t0 = __shfl_sync(0xFFFFFFFFu, p0, 31), t1 = __shfl_sync(0xFFFFFFFFu, p1, 31);
-            left0 = max(left0, t0);
-            left1 = max(left1, t1);
+            int L0 = __shfl_up_sync(0xFFFFFFFFu, p0, 1, SW), L1 = __shfl_up_sync(0xFFFFFFFFu, p1, 1, SW);
+            int R0 = __shfl_down_sync(0xFFFFFFFFu, s0, 1, SW), R1 = __shfl_down_sync(0xFFFFFFFFu, s1, 1, SW);
+            if (sl == 0) { L0 = NEG; L1 = NEG; }
+            if (sl == SW - 1) { R0 = POS; R1 = POS; }
+            L0 = max(L0, left0); L1 = max(L1, left1);
+            if (nchunks > 1) { R0 = min(R0, right_carry[wib][c][0]); R1 = min(R1, right_carry[wib][c][1]); }
+            left0 = max(left0, __shfl_sync(0xFFFFFFFFu, p0, SW - 1, SW));
+            left1 = max(left1, __shfl_sync(0xFFFFFFFFu, p1, SW - 1, SW));
+            if (!on) continue;
 
-            // emit: word q of the chunk, lane = bit
-            for (int q = 0; q < 32; q++) {
-                int kq = 32 * c + q;
-                if (kq >= ws) break;
-                uint32_t mq = __shfl_sync(0xFFFFFFFFu, m, q), lq = __shfl_sync(0xFFFFFFFFu, live, q);
-                int L0 = __shfl_sync(0xFFFFFFFFu, ex0, q), L1 = __shfl_sync(0xFFFFFFFFu, ex1, q);
-                int R0 = __shfl_sync(0xFFFFFFFFu, ey0, q), R1 = __shfl_sync(0xFFFFFFFFu, ey1, q);
-                int x = 32 * kq + lane;
-                if (x < w) {
-                    int s = (mq >> lane) & 1u;
-                    uint32_t opp = (s ? ~mq : mq) & lq;          // cells of the other state in the word
-                    int Lo = s ? L0 : L1, Ro = s ? R0 : R1;      // ... and outside it
-                    uint32_t below = opp & ((1u << lane) - 1u);
-                    uint32_t above = lane == 31 ? 0u : (opp & ~((2u << lane) - 1u));
-                    int lpos = below ? 32 * kq + 31 - __clz(below) : Lo;
-                    int rpos = above ? 32 * kq + __ffs(above) - 1 : Ro;
-                    int dist = min(x - lpos, rpos - x);
-                    uint32_t v = dist >= (int)kInf16 ? kInf16 : (uint32_t)dist;
-                    orow[x] = (uint16_t)(v | ((uint32_t)s << 15));
-                }
+            // cells past w continue the last live cell's run (no spurious run ends)
+            const int nlive = min(32, w - 32 * k);
+            const uint32_t lastbit = (m >> (nlive - 1)) & 1u;
+            const uint32_t me = (m & live) | (lastbit ? ~live : 0u);
+            const uint32_t tl = me ^ (me << 1);   // bit t: cell t starts a run (t >= 1)
+            const uint32_t tr = me ^ (me >> 1);   // bit t: cell t ends a run (t <= 30)
+            const int xb = 32 * k;
+            int runA = (me & 1u) ? L0 : L1;       // nearest other-state cell left of the run
+            int dl[32];
+#pragma unroll
+            for (int t = 0; t < 32; t++) {
+                if (t > 0 && ((tl >> t) & 1u)) runA = xb + t - 1;
+                dl[t] = xb + t - runA;
+            }
+            int runB = (me >> 31) ? R0 : R1;      // nearest other-state cell right of the run
+            uint32_t packed[16];
+#pragma unroll
+            for (int t = 31; t >= 0; t--) {
+                if (t < 31 && ((tr >> t) & 1u)) runB = xb + t + 1;
+                const int d = min(min(dl[t], runB - xb - t), (int)kInf16);
+                const uint32_t v = (uint32_t)d | (((me >> t) & 1u) << 15);
+                if (t & 1) packed[t >> 1] = v << 16;
+                else packed[t >> 1] |= v;
+            }
+            uint16_t* o = orow + xb;
+            if (vec_ok && nlive == 32) {
+                uint4* o4 = reinterpret_cast<uint4*>(o);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    o4[j] = make_uint4(packed[4 * j], packed[4 * j + 1], packed[4 * j + 2], packed[4 * j + 3]);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 32; t++)
+                    if (t < nlive) o[t] = (uint16_t)(packed[t >> 1] >> (16 * (t & 1)));
             }
         }
     }

@@ -118,6 +118,22 @@ def test_edt_mask_forms(dol, O, cuda, dims):
         same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
 
 
+@pytest.mark.parametrize("dims", [(8, 1000, 3), (16, 300, 37), (24, 5, 777), (8, 2049, 2), (40, 3, 1029),
+                                  (2000, 8), (64, 1027)])
+def test_edt_mask_long_lines(dol, O, cuda, dims):
+    """Long y / z lines: several TMA boxes, lengths off the 4 / 32 grid, runs
+    longer than a word, searches that reach the line ends."""
+    rng = np.random.default_rng(sum(dims) + 7)
+    big = np.float32(np.finfo(np.float32).max)
+    for p in (0.0, 0.0005, 0.01, 0.3, 0.97, 1.0):
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        b = O.mask_to_bool(m, dims)
+        want_sq = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SQUARED)), want_sq)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
+
+
 @pytest.mark.parametrize("dims", [(1, 1), (7, 1), (1, 7), (33, 17), (64, 48), (200, 130)])
 def test_felzenszwalb_float_field(dol, O, cuda, dims):
     """DOL::Felzenszwalb on arbitrary floats, not just 0 / FLT_MAX."""

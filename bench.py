@@ -340,6 +340,13 @@ def _config2(dol, torch, O, ref, res, L, sp):
         c2[f"{meth}_ms"] = _ev_ms(torch, run, 2) - _ev_ms(torch, lambda: work.copy_(bor), 2)
     out = dol.empty_field(dims)
     c2["felzenszwalb_sdf_ms"] = _ev_ms(torch, lambda: dol.edt_mask(md, dims, dol.EDT_SIGNED, out=out), 3)
+    # the tool's two-pass -S field: exterior + interior Danielsson (cw = 1), Dist(ext) - Dist(int)
+    tp_ws = torch.empty(L.dol_sdf_two_pass_workspace_size(n, n, n, dol.DANIELSSON), dtype=torch.uint8, device="cuda")
+    dol.sdf_two_pass(md, dims, "danielsson", want_deltas=False, workspace=tp_ws)
+    torch.cuda.synchronize()
+    c2["two_pass_danielsson_ms"] = _ev_ms(
+        torch, lambda: dol.sdf_two_pass(md, dims, "danielsson", want_deltas=False, workspace=tp_ws), 2)
+    del tp_ws
     if ref is not None:
         mh = md.cpu().numpy().view(np.uint32)
         b0 = O.border_init(mh, dims, use_ref=True)
@@ -347,6 +354,9 @@ def _config2(dol, torch, O, ref, res, L, sp):
             t0 = time.perf_counter()
             O.propagate(meth, b0, dims, 2, use_ref=True)
             c2[f"cpu_ref_{meth}_ms"] = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        O.sdf_two_pass(mh, dims, "danielsson", use_ref=True)
+        c2["cpu_ref_two_pass_danielsson_ms"] = (time.perf_counter() - t0) * 1e3
     res["signed_256"] = c2
 
 
@@ -443,8 +453,8 @@ def _config3(dol, torch, res, L, sp):
         t = _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)
         res["danielsson_3d_1024"] = {"workload": "1024^3 value noise, signed Danielsson deltas (cw=2)", "gpu_ms": t,
                                      "gvox_per_s": side ** 3 / t / 1e6,
-                                     "note": "serial in z and y (each slice needs the previous one after its full "
-                                             "2D sweep): one CTA, latency-bound"}
+                                     "note": "block schedule: exact fixed-point iteration over blocks of rows "
+                                             "(one cooperative launch per z direction), latency-bound"}
         del dv, mdv
 
 

@@ -67,6 +67,7 @@ def lib():
         for name in ("dol_mask_words", "dol_jumpflood_2d_workspace_size", "dol_jumpflood_3d_workspace_size",
                      "dol_fastsweep_3d_workspace_size", "dol_felzenszwalb_2d_workspace_size",
                      "dol_edt_mask_2d_workspace_size", "dol_edt_mask_3d_workspace_size", "dol_sdf_workspace_size",
+                     "dol_sdf_two_pass_workspace_size",
                      "dol_batch_workspace_size", "dol_sites_backward_workspace_size"):
             getattr(L, name).restype = C.c_size_t
         _lib = L
@@ -283,6 +284,26 @@ def sdf(mask, dims, method="danielsson", want_deltas=True, want_dist=True, works
         check(lib().dol_sdf_3d(*_ints(*dims), _ptr(mask), C.c_int(m), _ptr(dl), _ptr(df), _ptr(workspace),
                                C.c_size_t(wsb), _stream(stream)))
     return dl, df
+
+
+def sdf_two_pass(mask, dims, method="danielsson", want_deltas=True, want_dist=True, workspace=None, stream=None):
+    """Two-pass signed field (the tool's -S path, GenerateSignedDistance):
+    exterior deltas (to set cells), interior deltas (to clear cells), both with
+    cw = 1, and Dist(exterior) - Dist(interior).  Returns (exterior, interior,
+    dist); the deltas are None unless want_deltas."""
+    dims = _dims(dims)
+    m = METHODS.get(method, method)
+    de = empty_deltas(dims, mask.device) if want_deltas else None
+    di = empty_deltas(dims, mask.device) if want_deltas else None
+    df = empty_field(dims, mask.device) if want_dist else None
+    wsb = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    if len(dims) == 2:
+        check(lib().dol_sdf_two_pass_2d(*_ints(*dims), _ptr(mask), C.c_int(m), _ptr(de), _ptr(di), _ptr(df),
+                                        _ptr(workspace), C.c_size_t(wsb), _stream(stream)))
+    else:
+        check(lib().dol_sdf_two_pass_3d(*_ints(*dims), _ptr(mask), C.c_int(m), _ptr(de), _ptr(di), _ptr(df),
+                                        _ptr(workspace), C.c_size_t(wsb), _stream(stream)))
+    return de, di, df
 
 
 def sdf_host(mask_np, dims, method="danielsson", want_deltas=True, want_dist=True):

@@ -601,6 +601,81 @@ dol_status dol_sdf_3d(int w, int h, int d, const uint32_t* mask, int method, dol
     return sdf_common(3, w, h, d, mask, method, deltas, dist, workspace, workspace_bytes, stream);
 }
 
+// ---- two-pass signed fields (the tool's -S path) --------------------------------------------------
+
+size_t dol_sdf_two_pass_workspace_size(int w, int h, int d, int method)
+{
+    const int dim = d > 1 ? 3 : 2;
+    const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
+    const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
+    size_t b = 2 * align256(cells * cb);                    // exterior / interior deltas the caller does not keep
+    if (method == DOL_JUMPFLOOD) b += align256(cells * cb);  // ping-pong buffer
+    if (method == DOL_FASTSWEEP && dim == 3) b += align256(fastsweep3_workspace_bytes(w, h, d));
+    if (method == DOL_DANIELSSON) b += align256(danielsson_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
+    return b;
+}
+
+static dol_status sdf_two_pass_common(int dim, int w, int h, int d, const uint32_t* mask, int method, void* ext,
+                                      void* intr, float* dist, void* workspace, size_t workspace_bytes, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    if (ext) DOL_TRY(check_dev_ptr(ext, "exterior"));
+    if (intr) DOL_TRY(check_dev_ptr(intr, "interior"));
+    if (dist) DOL_TRY(check_dev_ptr(dist, "dist"));
+    if (!ext && !intr && !dist) return fail(DOL_ERR_INVALID_ARG, "at least one of exterior / interior / dist is required");
+    if (method != DOL_DANIELSSON && method != DOL_FASTSWEEP && method != DOL_JUMPFLOOD)
+        return fail(DOL_ERR_INVALID_ARG, "the two-pass field takes Danielsson, FastSweep or JumpFlood, not method %d",
+                    method);
+    if (method == DOL_DANIELSSON || method == DOL_FASTSWEEP) DOL_TRY(check_sweep_width(w));
+    if (method == DOL_FASTSWEEP && dim == 3 && w > kMaxSweepWidth3)
+        return fail(DOL_ERR_UNSUPPORTED, "3D FastSweep rows are limited to %d cells", kMaxSweepWidth3);
+    if (method == DOL_JUMPFLOOD && dim == 3 && d > 65535)
+        return fail(DOL_ERR_UNSUPPORTED, "JumpFlood volumes are limited to 65535 slices");
+    cudaStream_t st = S(stream);
+    const int dd = dim == 3 ? d : 1;
+    Workspace ws;
+    DOL_TRY(get_workspace(ws, workspace, workspace_bytes, dol_sdf_two_pass_workspace_size(w, h, dd, method), st));
+    const size_t cells = (size_t)w * h * dd;
+    const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
+    char* p = static_cast<char*>(ws.ptr);
+    void* de = ext ? ext : p;
+    p += align256(cells * cb);
+    void* di = intr ? intr : p;
+    p += align256(cells * cb);
+    const long long rows = (long long)h * dd;
+    launch_init_deltas(dim, mask, de, w, rows, 0, st);   // deltas to set cells
+    launch_init_deltas(dim, mask, di, w, rows, 1, st);   // deltas to clear cells
+    for (void* dl : {de, di}) {
+        if (method == DOL_DANIELSSON) {
+            run_danielsson(dim, dl, w, h, dd, 1, p, danielsson_workspace_bytes(dim, w, h, dd), ds->err_dev, st);
+        } else if (method == DOL_FASTSWEEP) {
+            if (dim == 2)
+                launch_fastsweep_2d(dl, w, h, 1, st);
+            else
+                launch_fastsweep_3d(dl, w, h, d, 1, p, ds->err_dev, st);
+        } else {
+            launch_jumpflood(dim, dl, p, w, h, dd, 1, st);
+        }
+    }
+    if (dist) launch_two_pass_dist(dim, de, di, dist, (long long)cells, st);
+    return launched("sdf_two_pass");
+}
+
+dol_status dol_sdf_two_pass_2d(int w, int h, const uint32_t* mask, int method, dol_delta2* exterior,
+                               dol_delta2* interior, float* dist, void* workspace, size_t workspace_bytes, void* stream)
+{
+    return sdf_two_pass_common(2, w, h, 1, mask, method, exterior, interior, dist, workspace, workspace_bytes, stream);
+}
+
+dol_status dol_sdf_two_pass_3d(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* exterior,
+                               dol_delta3* interior, float* dist, void* workspace, size_t workspace_bytes, void* stream)
+{
+    return sdf_two_pass_common(3, w, h, d, mask, method, exterior, interior, dist, workspace, workspace_bytes, stream);
+}
+
 // ---- batched signed fields ------------------------------------------------------------------------
 
 size_t dol_batch_workspace_size(int n)

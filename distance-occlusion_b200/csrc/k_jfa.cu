@@ -156,4 +156,37 @@ void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* 
         k_deltas_to_dist<3><<<grid, 256, 0, st>>>(deltas, cw, sign_mask, out, w, rows);
 }
 
+// ---- two-pass signed distance: Dist(exterior) - Dist(interior) ----
+// The tool's -S path (GenerateSignedDistance, DistanceOcclusionTool.cpp:1082-1123
+// 2D, :1197-1232 3D; Dist :54-61): deltas to set cells and deltas to clear cells,
+// each with cw = 1, give sqrtf of each squared length, subtracted in float.
+template <int kDim>
+__global__ void __launch_bounds__(256) k_two_pass_dist(const void* __restrict__ ext, const void* __restrict__ intr,
+                                                       float* __restrict__ out, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int32_t a, b;
+        if (kDim == 2) {
+            a = len(unpack2(__ldg(static_cast<const uint32_t*>(ext) + i)));
+            b = len(unpack2(__ldg(static_cast<const uint32_t*>(intr) + i)));
+        } else {
+            a = len(load3(static_cast<const int16_t*>(ext), i));
+            b = len(load3(static_cast<const int16_t*>(intr), i));
+        }
+        out[i] = __fsub_rn(sqrtf((float)a), sqrtf((float)b));
+    }
+}
+
+void launch_two_pass_dist(int dim, const void* ext, const void* intr, float* out, long long cells, cudaStream_t st)
+{
+    long long blocks = (cells + 255) / 256;
+    long long cap = (long long)g_num_sms * 32;
+    int grid = (int)(blocks < cap ? blocks : cap);
+    ProfScope ps("two_pass_dist", st);
+    if (dim == 2)
+        k_two_pass_dist<2><<<grid, 256, 0, st>>>(ext, intr, out, cells);
+    else
+        k_two_pass_dist<3><<<grid, 256, 0, st>>>(ext, intr, out, cells);
+}
+
 }  // namespace dolk

@@ -71,6 +71,7 @@ void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st);
 void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, int cw, cudaStream_t st);
 void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* sign_mask, float* out, int w, int h,
                            int d, cudaStream_t st);
+void launch_two_pass_dist(int dim, const void* ext, const void* intr, float* out, long long cells, cudaStream_t st);
 
 // k_sweep.cu -- Danielsson / FastSweep; `err` is a device int that receives a
 // non-zero code if a bounded wait gives up

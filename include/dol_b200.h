@@ -174,6 +174,19 @@ DOL_API dol_status dol_sdf_2d(int w, int h, const uint32_t* mask, int method, do
                       void* workspace, size_t workspace_bytes, void* stream);
 DOL_API dol_status dol_sdf_3d(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* deltas, float* dist,
                       void* workspace, size_t workspace_bytes, void* stream);
+/* Two-pass signed field (the tool's -S path, GenerateSignedDistance,
+   DistanceOcclusionTool.cpp:1082-1123 2D / :1197-1232 3D): deltas to set cells
+   (InitDeltasFromBitMask, invert = false) and to clear cells (invert = true),
+   each propagated by `method` (Danielsson, FastSweep or JumpFlood) with cw = 1;
+   dist = Dist(exterior) - Dist(interior) in cells (:54-61).  Any of exterior,
+   interior, dist may be NULL (not all three). */
+DOL_API size_t     dol_sdf_two_pass_workspace_size(int w, int h, int d, int method);
+DOL_API dol_status dol_sdf_two_pass_2d(int w, int h, const uint32_t* mask, int method, dol_delta2* exterior,
+                                       dol_delta2* interior, float* dist, void* workspace, size_t workspace_bytes,
+                                       void* stream);
+DOL_API dol_status dol_sdf_two_pass_3d(int w, int h, int d, const uint32_t* mask, int method, dol_delta3* exterior,
+                                       dol_delta3* interior, float* dist, void* workspace, size_t workspace_bytes,
+                                       void* stream);
 /* Same with HOST mask in and HOST outputs (either nullable); copies inside.
    Blocks until the result is in host memory. */
 DOL_API dol_status dol_sdf_2d_host(int w, int h, const uint32_t* mask, int method, dol_delta2* deltas, float* dist);

@@ -151,6 +151,17 @@ def deltas_to_dist(deltas, dims, cw, sign_mask=None):
     return out
 
 
+def sdf_two_pass(mask, dims, method, use_ref=False):
+    """The tool's -S field (GenerateSignedDistance, DistanceOcclusionTool.cpp:1082-1123
+    2D, :1197-1232 3D): deltas to set cells (InitDeltasFromBitMask, invert=false) and to
+    clear cells (invert=true), each through FindDeltas(method) with cw = 1 (:711-739),
+    then Dist(d0) - Dist(d1) in float (:54-61, :1136).  Returns (d0, d1, dist)."""
+    d0 = propagate(method, init_deltas(mask, dims, False, use_ref=use_ref), dims, 1, use_ref=use_ref)
+    d1 = propagate(method, init_deltas(mask, dims, True, use_ref=use_ref), dims, 1, use_ref=use_ref)
+    dist = (deltas_to_dist(d0, dims, 1) - deltas_to_dist(d1, dims, 1)).astype(np.float32)
+    return d0, d1, dist
+
+
 # ---- Felzenszwalb ---------------------------------------------------------------------
 
 def init_distances(mask, dims, use_ref=False):

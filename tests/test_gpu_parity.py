@@ -118,6 +118,25 @@ def test_edt_mask_forms(dol, O, cuda, dims):
         same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
 
 
+@pytest.mark.parametrize("method", ["danielsson", "fastsweep", "jumpflood"])
+@pytest.mark.parametrize("dims", [(1, 1), (31, 7), (64, 64), (100, 37), (257, 19), (1, 4, 3), (9, 7, 5), (33, 6, 5),
+                                  (24, 20, 16)])
+def test_sdf_two_pass(dol, O, cuda, dims, method):
+    """The tool's -S field: exterior and interior deltas bit-exact, Dist(ext) - Dist(int) identical floats."""
+    rng = np.random.default_rng(sum(dims) + len(method) + 5)
+    for p in PS:
+        m = rand_mask(O, rng, dims, p)
+        de, di, df = dol.sdf_two_pass(dev(cuda, m), dims, method)
+        dol.sync()
+        we, wi, wd = O.sdf_two_pass(m, dims, method)
+        np.testing.assert_array_equal(host(de), we, err_msg=f"exterior {method} p{p}")
+        np.testing.assert_array_equal(host(di), wi, err_msg=f"interior {method} p{p}")
+        same_float(host(df), wd)
+        _, _, only = dol.sdf_two_pass(dev(cuda, m), dims, method, want_deltas=False)
+        dol.sync()
+        same_float(host(only), wd)
+
+
 @pytest.mark.parametrize("dims", [(8, 1000, 3), (16, 300, 37), (24, 5, 777), (8, 2049, 2), (40, 3, 1029),
                                   (2000, 8), (64, 1027)])
 def test_edt_mask_long_lines(dol, O, cuda, dims):

@@ -143,6 +143,24 @@ def test_oracle_vs_reference_3d(O, dims):
             np.testing.assert_array_equal(O.felzenszwalb(f, dims), O.felzenszwalb(f, dims, use_ref=True))
 
 
+@pytest.mark.parametrize("dims", [(31, 9), (33, 11), (65, 20), (9, 7, 5), (33, 6, 5), (40, 1, 6)])
+def test_two_pass_oracle_vs_reference(O, dims):
+    """The -S field's deltas (exterior and interior, cw = 1) against the reference's
+    own init (both inversions) and delta methods; the float difference follows."""
+    if O.ref() is None:
+        pytest.skip("reference build (oracle/_ref) not available")
+    rng = np.random.default_rng(sum(dims) + 17)
+    for p in (0.0, 0.05, 0.3, 0.7, 1.0):
+        m = _rand_mask(rng, dims, p, True)
+        for meth in ("danielsson", "fastsweep", "jumpflood"):
+            mine, theirs = O.sdf_two_pass(m, dims, meth), O.sdf_two_pass(m, dims, meth, use_ref=True)
+            for a, b in zip(mine, theirs):
+                np.testing.assert_array_equal(a, b, err_msg=f"{meth} p{p}")
+            b = O.mask_to_bool(m, dims)
+            dist = mine[2]
+            assert (dist[b] <= 0).all() and (dist[~b] >= 0).all()
+
+
 def test_felzenszwalb_is_exact_edt(O):
     """The float envelope returns the exact squared EDT (so any exact EDT matches it)."""
     rng = np.random.default_rng(5)

@@ -319,6 +319,23 @@ def _config1(dol, torch, O, ref, res, dims):
         O.propagate("danielsson", ini, dims, 1, use_ref=True)
         c1["cpu_ref_ms"] = (time.perf_counter() - t0) * 1e3
     res["danielsson_2d_1024"] = c1
+    # Chamfer 3-4 on the same image, as the tool's GenerateDistanceChamfer (int16, INT16_MAX - 16)
+    f0 = dol.init_distances_int(md, dims, "int16", 32767 - 16)
+    f = f0.clone()
+    dol.chamfer(f, dims)
+    torch.cuda.synchronize()
+
+    def run_ch():
+        f.copy_(f0)
+        dol.chamfer(f, dims)
+    ch = {"workload": "1024^2, 100 points (seed 1), Chamfer 3-4 on int16",
+          "gpu_ms": _ev_ms(torch, run_ch, 5) - _ev_ms(torch, lambda: f.copy_(f0), 5)}
+    if ref is not None:
+        fi = O.init_distances_int(m, dims, np.int16, 32767 - 16, use_ref=True)
+        t0 = time.perf_counter()
+        O.chamfer(fi, dims, use_ref=True)
+        ch["cpu_ref_ms"] = (time.perf_counter() - t0) * 1e3
+    res["chamfer_2d_1024"] = ch
 
 
 def _config2(dol, torch, O, ref, res, L, sp):

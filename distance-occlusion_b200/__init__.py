@@ -183,6 +183,33 @@ def init_distances(mask, dims, max_d=None, stream=None):
     return out
 
 
+def init_distances_int(mask, dims, dtype="int16", max_d=None, out=None, stream=None):
+    """InitDistancesFromBitMask, int16 / int32 overloads: 0 on set bits, max_d elsewhere
+    (default INT16_MAX - 16 / INT32_MAX - 16, the margin the tool keeps for Chamfer's adds)."""
+    torch = _torch()
+    w, h = _dims(dims)
+    td = torch.int16 if str(dtype).endswith("int16") else torch.int32
+    if max_d is None:
+        max_d = 32767 - 16 if td == torch.int16 else 2**31 - 1 - 16
+    if out is None:
+        out = torch.empty((h, w), dtype=td, device=mask.device)
+    if td == torch.int16:
+        check(lib().dol_init_distances_2d_i16(*_ints(w, h), _ptr(mask), _ptr(out), C.c_int16(int(max_d)), _stream(stream)))
+    else:
+        check(lib().dol_init_distances_2d_i32(*_ints(w, h), _ptr(mask), _ptr(out), C.c_int32(int(max_d)), _stream(stream)))
+    return out
+
+
+def chamfer(dist, dims, stream=None):
+    """Chamfer 3-4 in place on an int16 / int32 field; returns the multiplier (3)."""
+    torch = _torch()
+    w, h = _dims(dims)
+    m = C.c_int(0)
+    fn = lib().dol_chamfer_2d_i16 if dist.dtype == torch.int16 else lib().dol_chamfer_2d_i32
+    check(fn(*_ints(w, h), _ptr(dist), C.byref(m), _stream(stream)))
+    return m.value
+
+
 def init_deltas(mask, dims, invert=False, out=None, stream=None):
     """InitDeltasFromBitMask."""
     dims = _dims(dims)

@@ -296,6 +296,54 @@ dol_status dol_pack_bytemask(int w, int h, int d, const uint8_t* bytes, int thre
 
 // ---- initialisation -------------------------------------------------------------------
 
+dol_status dol_init_distances_2d_i16(int w, int h, const uint32_t* mask, int16_t* dist, int16_t max_d, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    launch_init_distances_int<int16_t>(mask, dist, w, h, max_d, S(stream));
+    return launched("init_distances_2d_i16");
+}
+
+dol_status dol_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    launch_init_distances_int<int32_t>(mask, dist, w, h, max_d, S(stream));
+    return launched("init_distances_2d_i32");
+}
+
+static dol_status chamfer_common(int w, int h, void* dist, bool wide, int* multiplier, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    if (w < 2) return fail(DOL_ERR_UNSUPPORTED, "Chamfer needs rows of at least 2 cells (the reference reads outside a 1-cell row)");
+    DOL_TRY(check_sweep_width(w));
+    DOL_TRY(check_dev_ptr(dist, "dist"));
+    if (wide)
+        launch_chamfer_2d<int32_t>(static_cast<int32_t*>(dist), w, h, S(stream));
+    else
+        launch_chamfer_2d<int16_t>(static_cast<int16_t*>(dist), w, h, S(stream));
+    if (multiplier) *multiplier = 3;
+    return launched(wide ? "chamfer_2d_i32" : "chamfer_2d_i16");
+}
+
+dol_status dol_chamfer_2d_i16(int w, int h, int16_t* dist, int* multiplier, void* stream)
+{
+    return chamfer_common(w, h, dist, false, multiplier, stream);
+}
+
+dol_status dol_chamfer_2d_i32(int w, int h, int32_t* dist, int* multiplier, void* stream)
+{
+    return chamfer_common(w, h, dist, true, multiplier, stream);
+}
+
 dol_status dol_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, float max_d, void* stream)
 {
     DeviceState* ds;

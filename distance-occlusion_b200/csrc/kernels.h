@@ -96,6 +96,12 @@ void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t
                       int* counter, cudaStream_t st);
 void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, int* err, cudaStream_t st);
 
+// k_chamfer.cu -- Chamfer 3-4 on int16 / int32 fields (one CTA walks the rows)
+template <typename T>
+void launch_chamfer_2d(T* dist, int w, int h, cudaStream_t st);
+template <typename T>
+void launch_init_distances_int(const uint32_t* mask, T* dist, int w, long long rows, T max_d, cudaStream_t st);
+
 // k_sites.cu
 void launch_sites_seed(int dim, int w, int h, int d, int n, const float* sites, uint32_t* mask, int* cell_site,
                        cudaStream_t st);

@@ -91,6 +91,38 @@ namespace DOL
         df.down(distances, (size_t)w * h * sizeof(float));
     }
 
+    void InitDistancesFromBitMask(int w, int h, const uint32_t mask[], int16_t distances[], int16_t maxD)
+    {
+        Dev dm(MaskBytes(w, h, 1)), df((size_t)w * h * sizeof(int16_t));
+        dm.up(mask, MaskBytes(w, h, 1));
+        Check(dol_init_distances_2d_i16(w, h, dm.as<uint32_t>(), df.as<int16_t>(), maxD, nullptr));
+        Finish();
+        df.down(distances, (size_t)w * h * sizeof(int16_t));
+    }
+
+    void InitDistancesFromBitMask(int w, int h, const uint32_t mask[], int32_t distances[], int32_t maxD)
+    {
+        Dev dm(MaskBytes(w, h, 1)), df((size_t)w * h * sizeof(int32_t));
+        dm.up(mask, MaskBytes(w, h, 1));
+        Check(dol_init_distances_2d_i32(w, h, dm.as<uint32_t>(), df.as<int32_t>(), maxD, nullptr));
+        Finish();
+        df.down(distances, (size_t)w * h * sizeof(int32_t));
+    }
+
+    int Chamfer(int w, int h, int16_t distances[])
+    {
+        int m = 3;
+        InPlace(distances, (size_t)w * h, [&](int16_t* d) { Check(dol_chamfer_2d_i16(w, h, d, &m, nullptr)); });
+        return m;
+    }
+
+    int Chamfer(int w, int h, int32_t distances[])
+    {
+        int m = 3;
+        InPlace(distances, (size_t)w * h, [&](int32_t* d) { Check(dol_chamfer_2d_i32(w, h, d, &m, nullptr)); });
+        return m;
+    }
+
     void Felzenszwalb(int w, int h, float distances[])
     {
         InPlace(distances, (size_t)w * h, [&](float* d) { Check(dol_felzenszwalb_2d(w, h, d, nullptr, 0, nullptr)); });

@@ -52,7 +52,11 @@ namespace DOL
     const int16_t kMaxDelta3 = 25000;
 
     // --- distances -----------------------------------------------------------------
+    void InitDistancesFromBitMask(int w, int h, const uint32_t mask[], int16_t distances[], int16_t maxD = INT16_MAX);
+    void InitDistancesFromBitMask(int w, int h, const uint32_t mask[], int32_t distances[], int32_t maxD = INT32_MAX);
     void InitDistancesFromBitMask(int w, int h, const uint32_t mask[], float distances[], float maxD = FLT_MAX);
+    int  Chamfer(int w, int h, int16_t distances[]);   // returns the multiplier (3)
+    int  Chamfer(int w, int h, int32_t distances[]);
     void Felzenszwalb(int w, int h, float distances[]);   // squared distances, in place
 
     // --- delta methods --------------------------------------------------------------

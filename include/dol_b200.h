@@ -102,6 +102,11 @@ DOL_API dol_status dol_pack_bytemask(int w, int h, int d, const uint8_t* bytes, 
 /* ---- initialisation ------------------------------------------------------------ */
 /* InitDistancesFromBitMask(float) (DistanceOcclusionLib.cpp:211-222): 0 on set bits, max_d elsewhere */
 DOL_API dol_status dol_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, float max_d, void* stream);
+/* InitDistancesFromBitMask(int16_t / int32_t) (DistanceOcclusionLib.cpp:203-214, header :60-61) */
+DOL_API dol_status dol_init_distances_2d_i16(int w, int h, const uint32_t* mask, int16_t* dist, int16_t max_d,
+                                             void* stream);
+DOL_API dol_status dol_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d,
+                                             void* stream);
 /* InitDeltasFromBitMask (DistanceOcclusionLib.cpp:224-254, :1289-1321) */
 DOL_API dol_status dol_init_deltas_2d(int w, int h, const uint32_t* mask, dol_delta2* deltas, int invert, void* stream);
 DOL_API dol_status dol_init_deltas_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, int invert, void* stream);
@@ -126,6 +131,16 @@ DOL_API dol_status dol_jumpflood_2d(int w, int h, dol_delta2* deltas, int cw,
                             void* workspace, size_t workspace_bytes, void* stream);
 DOL_API dol_status dol_jumpflood_3d(int w, int h, int d, dol_delta3* deltas, int cw,
                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Chamfer 3-4 (integer distances, in place) ------------------------------------------ */
+/* Chamfer(w, h, int16_t[] / int32_t[]) (DistanceOcclusionLib.cpp:916-1016, header :66-67):
+   one raster pass down and one up with edge cost 3 and diagonal cost 4.
+   *multiplier (nullable, host) receives 3: divide by it for cells.  Rows of at
+   least 2 and at most 4096 cells.  int32 fields: results equal the reference's
+   while every input is at most INT32_MAX - 4 (beyond that the reference's own
+   int32 sums wrap). */
+DOL_API dol_status dol_chamfer_2d_i16(int w, int h, int16_t* dist, int* multiplier, void* stream);
+DOL_API dol_status dol_chamfer_2d_i32(int w, int h, int32_t* dist, int* multiplier, void* stream);
 
 /* ---- Felzenszwalb ------------------------------------------------------------------- */
 /* Felzenszwalb(w,h,float[]) (DistanceOcclusionLib.cpp:1065-1085): in-place squared

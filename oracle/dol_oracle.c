@@ -156,6 +156,78 @@ void dolo_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, flo
             dist[(size_t)y * w + x] = mask_bit(mask + (size_t)y * ws, x) ? 0.0f : max_d;
 }
 
+void dolo_init_distances_2d_i16(int w, int h, const uint32_t* mask, i16* dist, i16 max_d)
+{
+    /* InitFromBitMask<int16_t>, :183-222 */
+    int ws = words_per_row(w);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++)
+            dist[(size_t)y * w + x] = mask_bit(mask + (size_t)y * ws, x) ? 0 : max_d;
+}
+
+void dolo_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d)
+{
+    /* InitFromBitMask<int32_t>, :183-222 */
+    int ws = words_per_row(w);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++)
+            dist[(size_t)y * w + x] = mask_bit(mask + (size_t)y * ws, x) ? 0 : max_d;
+}
+
+/* Chamfer 3-4 (Borgefors), :916-1004.  One raster pass down the rows (row 0:
+ * left neighbour only; other rows: the three cells above, then the left
+ * neighbour) and one pass up (mirrored).  A cell takes a neighbour's value plus
+ * 3 (edge) or 4 (diagonal) when that is smaller.  Sums are int (int16 values
+ * are promoted, so they never wrap); int32 sums wrap as two's complement, which
+ * is what the reference's build does past INT32_MAX (done here in uint32 to
+ * stay defined).  Rows of one cell are not handled (the reference reads
+ * outside the row there).  Returns the multiplier 3. */
+#define CHAMFER_BODY(T, ADD)                                                               \
+    const int d0 = 3, d1 = 4;                                                              \
+    T* row0 = dist;                                                                        \
+    for (int x = 1; x < w; x++)                                                            \
+        if (row0[x] > ADD(row0[x - 1], d0)) row0[x] = (T)ADD(row0[x - 1], d0);             \
+    for (int y = 1; y < h; y++) {                                                          \
+        T* row1 = row0 + w;                                                                \
+        if (row1[0] > ADD(row0[0], d0)) row1[0] = (T)ADD(row0[0], d0);                     \
+        if (row1[0] > ADD(row0[1], d1)) row1[0] = (T)ADD(row0[1], d1);                     \
+        for (int x = 1; x < w - 1; x++) {                                                  \
+            if (row1[x] > ADD(row0[x - 1], d1)) row1[x] = (T)ADD(row0[x - 1], d1);         \
+            if (row1[x] > ADD(row0[x], d0)) row1[x] = (T)ADD(row0[x], d0);                 \
+            if (row1[x] > ADD(row0[x + 1], d1)) row1[x] = (T)ADD(row0[x + 1], d1);         \
+            if (row1[x] > ADD(row1[x - 1], d0)) row1[x] = (T)ADD(row1[x - 1], d0);         \
+        }                                                                                  \
+        if (row1[w - 1] > ADD(row0[w - 2], d1)) row1[w - 1] = (T)ADD(row0[w - 2], d1);     \
+        if (row1[w - 1] > ADD(row0[w - 1], d0)) row1[w - 1] = (T)ADD(row0[w - 1], d0);     \
+        if (row1[w - 1] > ADD(row1[w - 2], d0)) row1[w - 1] = (T)ADD(row1[w - 2], d0);     \
+        row0 = row1;                                                                       \
+    }                                                                                      \
+    row0 = dist + (size_t)h * w - w;                                                       \
+    for (int x = w - 2; x >= 0; x--)                                                       \
+        if (row0[x] > ADD(row0[x + 1], d0)) row0[x] = (T)ADD(row0[x + 1], d0);             \
+    for (int y = h - 2; y >= 0; y--) {                                                     \
+        T* row1 = row0 - w;                                                                \
+        if (row1[w - 1] > ADD(row0[w - 1], d0)) row1[w - 1] = (T)ADD(row0[w - 1], d0);     \
+        if (row1[w - 1] > ADD(row0[w - 2], d1)) row1[w - 1] = (T)ADD(row0[w - 2], d1);     \
+        for (int x = w - 2; x > 0; x--) {                                                  \
+            if (row1[x] > ADD(row0[x + 1], d1)) row1[x] = (T)ADD(row0[x + 1], d1);         \
+            if (row1[x] > ADD(row0[x], d0)) row1[x] = (T)ADD(row0[x], d0);                 \
+            if (row1[x] > ADD(row0[x - 1], d1)) row1[x] = (T)ADD(row0[x - 1], d1);         \
+            if (row1[x] > ADD(row1[x + 1], d0)) row1[x] = (T)ADD(row1[x + 1], d0);         \
+        }                                                                                  \
+        if (row1[0] > ADD(row0[1], d1)) row1[0] = (T)ADD(row0[1], d1);                     \
+        if (row1[0] > ADD(row0[0], d0)) row1[0] = (T)ADD(row0[0], d0);                     \
+        if (row1[0] > ADD(row1[1], d0)) row1[0] = (T)ADD(row1[1], d0);                     \
+        row0 = row1;                                                                       \
+    }                                                                                      \
+    return d0;
+
+#define ADD16(a, b) ((int)(a) + (b))
+#define ADD32(a, b) ((int32_t)((uint32_t)(a) + (uint32_t)(b)))
+
+int dolo_chamfer_2d_i16(int w, int h, i16* dist) { CHAMFER_BODY(i16, ADD16) }
+int dolo_chamfer_2d_i32(int w, int h, int32_t* dist) { CHAMFER_BODY(int32_t, ADD32) }
+
 void dolo_init_deltas_2d(int w, int h, const uint32_t* mask, i16* deltas, int invert)
 {
     /* :224-254 -- zero where (bit ^ invert), kMaxDelta2 elsewhere */

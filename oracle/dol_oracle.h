@@ -42,6 +42,10 @@ void dolo_pack_bytes(int w, int h, const uint8_t* img, int threshold, int less_t
 
 /* initialisation (DistanceOcclusionLib.cpp:183-254, 1289-1321) */
 void dolo_init_distances_2d(int w, int h, const uint32_t* mask, float* dist, float max_d);
+void dolo_init_distances_2d_i16(int w, int h, const uint32_t* mask, int16_t* dist, int16_t max_d);
+void dolo_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d);
+int dolo_chamfer_2d_i16(int w, int h, int16_t* dist);
+int dolo_chamfer_2d_i32(int w, int h, int32_t* dist);
 void dolo_init_deltas_2d(int w, int h, const uint32_t* mask, int16_t* deltas, int invert);
 void dolo_init_deltas_3d(int w, int h, int d, const uint32_t* mask, int16_t* deltas, int invert);
 

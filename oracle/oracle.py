@@ -162,6 +162,31 @@ def sdf_two_pass(mask, dims, method, use_ref=False):
     return d0, d1, dist
 
 
+# ---- Chamfer (integer distances) ----------------------------------------------------------
+
+def init_distances_int(mask, dims, dtype, max_d, use_ref=False):
+    """InitDistancesFromBitMask, int16 / int32 overloads (DistanceOcclusionLib.cpp:183-222)."""
+    w, h = dims
+    dt = np.dtype(dtype)
+    out = np.empty((h, w), dtype=dt)
+    tag = "i16" if dt == np.int16 else "i32"
+    cval = C.c_int16(int(max_d)) if dt == np.int16 else C.c_int32(int(max_d))
+    getattr(ref() if use_ref else lib(), ("ref_" if use_ref else "dolo_") + f"init_distances_2d_{tag}")(
+        *_i(w, h), _p(mask), _p(out), cval)
+    return out
+
+
+def chamfer(dist, dims, use_ref=False):
+    """Chamfer 3-4 on a copy of an int16 / int32 field (DistanceOcclusionLib.cpp:916-1016);
+    returns (field, multiplier)."""
+    w, h = dims
+    out = np.ascontiguousarray(dist).copy()
+    tag = "i16" if out.dtype == np.int16 else "i32"
+    m = getattr(ref() if use_ref else lib(), ("ref_" if use_ref else "dolo_") + f"chamfer_2d_{tag}")(
+        *_i(w, h), _p(out))
+    return out, m
+
+
 # ---- Felzenszwalb ---------------------------------------------------------------------
 
 def init_distances(mask, dims, use_ref=False):

@@ -40,6 +40,10 @@ void ref_jumpflood_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::
 void ref_bruteforce_2d(int w, int h, DOL::cCellDelta2* dl, int cw) { DOL::BruteForce(w, h, dl, cw); }
 void ref_bruteforce_3d(int w, int h, int d, DOL::cCellDelta3* dl, int cw) { DOL::BruteForce(w, h, d, dl, cw); }
 void ref_felzenszwalb_2d(int w, int h, float* dist) { DOL::Felzenszwalb(w, h, dist); }
+void ref_init_distances_2d_i16(int w, int h, const uint32_t* mask, int16_t* dist, int16_t max_d) { DOL::InitDistancesFromBitMask(w, h, mask, dist, max_d); }
+void ref_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d) { DOL::InitDistancesFromBitMask(w, h, mask, dist, max_d); }
+int ref_chamfer_2d_i16(int w, int h, int16_t* dist) { return DOL::Chamfer(w, h, dist); }
+int ref_chamfer_2d_i32(int w, int h, int32_t* dist) { return DOL::Chamfer(w, h, dist); }
 
 /* 3D restatement on the reference's own 1D routine: z, then y, then x.  Lines
  * are split over `threads` host threads, each with private v/z/line scratch

@@ -1,8 +1,10 @@
 // Exercises the C++ host interface (namespace DOL, shim/DistanceOcclusionB200.h)
 // the way the reference's tool drives DistanceOcclusionLib: make a mask, run a
 // delta method, write the result.  Usage:
-//   shim_driver <method 0|1|2> <signed 0|1> <w> <h> <d> <points> <seed> <out.bin>
-// d = 0 selects 2D.  The output is the raw delta array (cCellDelta2/3 bytes).
+//   shim_driver <method 0|1|2|4> <signed 0|1> <w> <h> <d> <points> <seed> <out.bin>
+// d = 0 selects 2D.  The output is the raw delta array (cCellDelta2/3 bytes);
+// method 4 (Chamfer, 2D only, as the tool's GenerateDistanceChamfer) writes the
+// int16 distances instead.
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -21,7 +23,16 @@ int main(int argc, char** argv)
     FILE* f = fopen(argv[8], "wb");
     if (!f) return 3;
     try {
-        if (d == 0) {
+        if (d == 0 && method == 4) {
+            uint32_t* mask = CreateBitMask(w, h);
+            BitMaskAddBlock(w, h, 4, mask);
+            BitMaskAddPoints(w, h, points, seed, mask);
+            std::vector<int16_t> dist((size_t)w * h);
+            InitDistancesFromBitMask(w, h, mask, dist.data(), (int16_t)(INT16_MAX - 16));
+            if (Chamfer(w, h, dist.data()) != 3) return 4;
+            fwrite(dist.data(), sizeof(int16_t), dist.size(), f);
+            DestroyBitMask(mask);
+        } else if (d == 0) {
             uint32_t* mask = CreateBitMask(w, h);
             BitMaskAddBlock(w, h, 4, mask);
             BitMaskAddPoints(w, h, points, seed, mask);

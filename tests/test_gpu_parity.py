@@ -137,6 +137,42 @@ def test_sdf_two_pass(dol, O, cuda, dims, method):
         same_float(host(only), wd)
 
 
+@pytest.mark.parametrize("dims", [(2, 1), (2, 9), (3, 1), (31, 7), (64, 64), (100, 37), (257, 19), (1000, 5),
+                                  (4096, 3), (33, 300)])
+def test_chamfer(dol, O, cuda, dims):
+    """Chamfer 3-4 on int16 and int32 fields against the oracle, bit for bit: the
+    tool's init (INT16_MAX - 16), masks of every density, and arbitrary values
+    (int16: the whole range; int32: up to INT32_MAX - 4, where the reference's
+    own sums stop wrapping)."""
+    import torch
+    rng = np.random.default_rng(sum(dims) + 41)
+    for p in PS:
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        for dt, tdt, mx in ((np.int16, torch.int16, 32767 - 16), (np.int32, torch.int32, 2**31 - 1 - 16)):
+            f = dol.init_distances_int(md, dims, dtype=str(tdt), max_d=mx)
+            want_f = O.init_distances_int(m, dims, dt, mx)
+            np.testing.assert_array_equal(f.cpu().numpy(), want_f)
+            assert dol.chamfer(f, dims) == 3
+            dol.sync()
+            np.testing.assert_array_equal(f.cpu().numpy(), O.chamfer(want_f, dims)[0], err_msg=f"{dt} p{p}")
+    shape = tuple(reversed(dims))
+    for dt, lo, hi in ((np.int16, -32768, 32767), (np.int32, -2**31, 2**31 - 1 - 4)):
+        f = rng.integers(lo, hi, size=shape, dtype=np.int64, endpoint=True).astype(dt)
+        t = torch.from_numpy(f.copy()).cuda()
+        dol.chamfer(t, dims)
+        dol.sync()
+        np.testing.assert_array_equal(t.cpu().numpy(), O.chamfer(f, dims)[0], err_msg=f"arbitrary {dt}")
+
+
+def test_chamfer_rejects_bad_widths(dol, cuda):
+    import torch
+    for w in (1, 4097):
+        t = torch.zeros((3, w), dtype=torch.int16, device="cuda")
+        with pytest.raises(dol.DolError):
+            dol.chamfer(t, (w, 3))
+
+
 @pytest.mark.parametrize("dims", [(8, 1000, 3), (16, 300, 37), (24, 5, 777), (8, 2049, 2), (40, 3, 1029),
                                   (2000, 8), (64, 1027)])
 def test_edt_mask_long_lines(dol, O, cuda, dims):

@@ -161,6 +161,27 @@ def test_two_pass_oracle_vs_reference(O, dims):
             assert (dist[b] <= 0).all() and (dist[~b] >= 0).all()
 
 
+@pytest.mark.parametrize("dims", [(2, 1), (2, 6), (7, 1), (31, 9), (33, 17), (100, 3), (65, 64)])
+def test_chamfer_oracle_vs_reference(O, dims):
+    """Chamfer on int16 / int32 fields: tool-style inits, the int32 default that
+    wraps in the reference, and arbitrary values (negative and near the maximum)."""
+    if O.ref() is None:
+        pytest.skip("reference build (oracle/_ref) not available")
+    rng = np.random.default_rng(sum(dims) + 23)
+    for p in (0.0, 0.01, 0.2, 0.9):
+        m = _rand_mask(rng, dims, p, True)
+        for dt, md in ((np.int16, 32767 - 16), (np.int16, 32767), (np.int32, 2**31 - 16), (np.int32, 2**31 - 1)):
+            f = O.init_distances_int(m, dims, dt, md)
+            np.testing.assert_array_equal(f, O.init_distances_int(m, dims, dt, md, use_ref=True))
+            (a, ma), (b, mb) = O.chamfer(f, dims), O.chamfer(f, dims, use_ref=True)
+            assert ma == mb == 3
+            np.testing.assert_array_equal(a, b, err_msg=f"{dt} {md} p{p}")
+    for dt in (np.int16, np.int32):
+        info = np.iinfo(dt)
+        f = rng.integers(info.min, info.max, size=tuple(reversed(dims)), dtype=np.int64, endpoint=True).astype(dt)
+        np.testing.assert_array_equal(O.chamfer(f, dims)[0], O.chamfer(f, dims, use_ref=True)[0])
+
+
 def test_felzenszwalb_is_exact_edt(O):
     """The float envelope returns the exact squared EDT (so any exact EDT matches it)."""
     rng = np.random.default_rng(5)

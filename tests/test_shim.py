@@ -41,3 +41,19 @@ def test_shim_matches_oracle(driver, O, tmp_path, method, sgn, dims):
     start = O.border_init(m, shape) if sgn else O.init_deltas(m, shape)
     want = O.propagate(["danielsson", "fastsweep", "jumpflood"][method], start, shape, 2 if sgn else 1)
     np.testing.assert_array_equal(got, want.reshape(-1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(70, 45), (300, 7)])
+def test_shim_chamfer_matches_oracle(driver, O, tmp_path, dims):
+    """DOL::InitDistancesFromBitMask(int16) + DOL::Chamfer, as GenerateDistanceChamfer calls them."""
+    w, h = dims
+    out = tmp_path / "out.bin"
+    subprocess.run([driver, "4", "0", str(w), str(h), "0", "40", "9", str(out)], check=True)
+    got = np.fromfile(out, dtype=np.int16)
+    m = O.new_mask(w, h)
+    O.add_block(m, dims, 4)
+    O.add_points(m, dims, 40, 9)
+    want, mult = O.chamfer(O.init_distances_int(m, dims, np.int16, 32767 - 16), dims)
+    assert mult == 3
+    np.testing.assert_array_equal(got, want.reshape(-1))

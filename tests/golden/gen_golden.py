@@ -7,7 +7,17 @@ DistanceOcclusionLib.cpp as it lies).  Small cases are stored whole
 (golden_small.npz); configuration-sized cases as SHA-256 digests of the output
 bytes (golden_digests.json), which keeps the fixtures a few hundred KB.
 
-    python tests/golden/gen_golden.py
+    python tests/golden/gen_golden.py            # small cases, 1024^2 and 64^3 digests
+    python tests/golden/gen_golden.py --full     # adds the benchmarked sizes (a few minutes, ~20 GB RAM)
+
+--full digests the reference's outputs on the two benchmarked volumes, from
+the same synthetic masks the library generates (its host generator; the
+mask digests pin host and device generation to each other):
+  1024^3 value noise (lattice 16, seed 3): signed Felzenszwalb SDF (the
+      reference's 1D routine along z, y, x for each sign, sqrt, difference)
+      and signed Danielsson deltas (border init, cw = 2);
+  256^3, 32 boxes + 32 spheres (sides / radii 4-40, seed 7): border init,
+      Danielsson / FastSweep / JumpFlood with cw = 2, signed Felzenszwalb SDF.
 """
 import hashlib
 import json
@@ -95,9 +105,57 @@ def main():
     ini = O.init_deltas(m, dims, use_ref=True)
     for meth in ("danielsson", "fastsweep", "jumpflood"):
         dig[f"v64_{meth}_cw1"] = digest(O.propagate(meth, ini, dims, 1, use_ref=True))
+    if "--full" in sys.argv:
+        dig.update(full_size())
+    else:
+        with open(os.path.join(HERE, "golden_digests.json")) as f:
+            old = json.load(f)
+        dig.update({k: v for k, v in old.items() if k.startswith(("c2_", "c3_"))})
     with open(os.path.join(HERE, "golden_digests.json"), "w") as f:
         json.dump(dig, f, indent=1, sort_keys=True)
     print("wrote", len(small), "arrays and", len(dig), "digests")
+
+
+def _signed_felz_ref(m, dims, threads):
+    b = O.mask_to_bool(m, dims)
+    big = np.float32(np.finfo(np.float32).max)
+    e_occ = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims, use_ref=True, threads=threads)
+    e_emp = O.felzenszwalb(np.where(b, big, np.float32(0)).astype(np.float32), dims, use_ref=True, threads=threads)
+    del b
+    return (np.sqrt(e_occ) - np.sqrt(e_emp)).astype(np.float32)
+
+
+def full_size():
+    import ctypes as C
+    sys.path.insert(0, ROOT)
+    import bench
+    L = bench.load_dol().lib()
+    threads = os.cpu_count() or 1
+    dig = {}
+    # 256^3 shapes
+    n = 256
+    dims = (n, n, n)
+    m = np.zeros(O.mask_words(*dims), np.uint32)
+    L.dol_gen_shapes_3d_host(n, n, n, 32, 32, 4, 40, C.c_uint32(7), m.ctypes.data_as(C.c_void_p))
+    dig["c2_mask"] = digest(m)
+    bor = O.border_init(m, dims, use_ref=True)
+    dig["c2_border"] = digest(bor)
+    for meth in ("danielsson", "fastsweep", "jumpflood"):
+        dig[f"c2_{meth}_cw2"] = digest(O.propagate(meth, bor, dims, 2, use_ref=True))
+        print("c2", meth, flush=True)
+    dig["c2_felz_signed"] = digest(_signed_felz_ref(m, dims, threads))
+    # 1024^3 value noise
+    n = 1024
+    dims = (n, n, n)
+    m = np.zeros(O.mask_words(*dims), np.uint32)
+    L.dol_gen_value_noise_3d_host(n, n, n, 16, C.c_uint32(3), m.ctypes.data_as(C.c_void_p))
+    dig["c3_mask"] = digest(m)
+    dig["c3_felz_signed"] = digest(_signed_felz_ref(m, dims, threads))
+    print("c3 felzenszwalb", flush=True)
+    bor = O.border_init(m, dims, use_ref=True)
+    dig["c3_danielsson_cw2"] = digest(O.propagate("danielsson", bor, dims, 2, use_ref=True))
+    print("c3 danielsson", flush=True)
+    return dig
 
 
 if __name__ == "__main__":

@@ -21,6 +21,8 @@ The directory name contains a hyphen, so import it by path::
 from __future__ import annotations
 
 import ctypes as C
+
+import numpy as np
 import os
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -286,6 +288,17 @@ def edt_mask(mask, dims, form=EDT_DIST, out=None, workspace=None, stream=None):
     else:
         check(lib().dol_edt_mask_3d(*_ints(*dims), _ptr(mask), _ptr(out), C.c_int(form), _ptr(workspace),
                                     C.c_size_t(wsb), _stream(stream)))
+    return out
+
+
+def edt_mask_host(mask_np, dims, form=EDT_DIST):
+    """Mask-driven 3D EDT with host buffers (dol_edt_mask_3d_host): numpy mask in,
+    numpy float32 field out; the copy back overlaps the last pass."""
+    w, h, d = _dims(dims)
+    m = np.ascontiguousarray(mask_np, dtype=np.uint32)
+    out = np.empty((d, h, w), dtype=np.float32)
+    check(lib().dol_edt_mask_3d_host(*_ints(w, h, d), C.c_void_p(m.ctypes.data), C.c_void_p(out.ctypes.data),
+                                     C.c_int(form)))
     return out
 
 

@@ -988,24 +988,80 @@ dol_status dol_sdf_3d_host(int w, int h, int d, const uint32_t* mask, int method
     return sdf_host(3, w, h, d, mask, method, deltas, dist);
 }
 
+// The z pass runs in y chunks; each chunk's rows go back to the host on a
+// second stream while the next chunk computes (cudaMemcpy2DAsync: the chunk's
+// rows of every slice, one slice pitch apart).
+struct ChunkCopy {
+    float* host;
+    const float* dev;
+    int w, h, d;
+    cudaStream_t compute, copy;
+    cudaEvent_t ev[16];
+    int n;
+    cudaError_t err;
+};
+
+static void chunk_done(void* ctx, int y0, int y1)
+{
+    ChunkCopy* cc = static_cast<ChunkCopy*>(ctx);
+    if (cc->err != cudaSuccess || cc->n >= 16) return;
+    cudaEvent_t e = cc->ev[cc->n++];
+    const size_t pitch = (size_t)cc->w * cc->h * sizeof(float);
+    const size_t first = (size_t)y0 * cc->w;
+    cudaError_t r = cudaEventRecord(e, cc->compute);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(cc->copy, e, 0);
+    if (r == cudaSuccess)
+        r = cudaMemcpy2DAsync(cc->host + first, pitch, cc->dev + first, pitch, (size_t)(y1 - y0) * cc->w * sizeof(float),
+                              (size_t)cc->d, cudaMemcpyDeviceToHost, cc->copy);
+    if (r != cudaSuccess) cc->err = r;
+}
+
 dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float* out, int form)
 {
     DeviceState* ds;
     DOL_TRY(device_state(&ds));
     DOL_TRY(check_dims(w, h, d));
     if (!mask || !out) return fail(DOL_ERR_INVALID_ARG, "mask and out are required");
-    OwnStream os;
-    if (cudaStreamCreateWithFlags(&os.st, cudaStreamNonBlocking) != cudaSuccess)
+    if (form != DOL_EDT_SQUARED && form != DOL_EDT_DIST && form != DOL_EDT_SIGNED)
+        return fail(DOL_ERR_INVALID_ARG, "form must be DOL_EDT_SQUARED, DOL_EDT_DIST or DOL_EDT_SIGNED");
+    if (w > 16384 || h > 16384 || d > 16384) return fail(DOL_ERR_UNSUPPORTED, "EDT dimensions are limited to 16384");
+    OwnStream os, cs;
+    if (cudaStreamCreateWithFlags(&os.st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&cs.st, cudaStreamNonBlocking) != cudaSuccess)
         return fail(DOL_ERR_CUDA, "cudaStreamCreate failed");
     const size_t cells = (size_t)w * h * d;
     const size_t mb = dol_mask_words(w, h, d) * sizeof(uint32_t);
-    DevBuf dm, df;
+    DevBuf dm, df, dw;
     DOL_TRY(dm.alloc(mb, os.st));
     DOL_TRY(df.alloc(cells * sizeof(float), os.st));
+    DOL_TRY(dw.alloc(edt_workspace_bytes(3, w, h, d), os.st));
     DOL_TRY(copy(dm.p, mask, mb, cudaMemcpyHostToDevice, os.st));
-    DOL_TRY(edt_common(3, w, h, d, static_cast<uint32_t*>(dm.p), static_cast<float*>(df.p), form, nullptr, 0, os.st));
-    DOL_TRY(copy(out, df.p, cells * sizeof(float), cudaMemcpyDeviceToHost, os.st));
-    return dol_sync(os.st);
+    ChunkCopy cc{out, static_cast<const float*>(df.p), w, h, d, os.st, cs.st, {}, 0, cudaSuccess};
+    const int chunks = h >= 64 ? 8 : 1;
+    for (int i = 0; i < chunks; i++)
+        if (cudaEventCreateWithFlags(&cc.ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            for (int j = 0; j < i; j++) cudaEventDestroy(cc.ev[j]);
+            return fail(DOL_ERR_CUDA, "cudaEventCreate failed");
+        }
+    launch_edt_mask_3d_chunked(static_cast<uint32_t*>(dm.p), static_cast<float*>(df.p), w, h, d, form, dw.p,
+                               ds->err_dev, os.st, chunks, chunk_done, &cc);
+    const cudaError_t le = cudaGetLastError();
+    // the copies must finish before the device buffers are released (the
+    // DevBuf destructors free on the compute stream)
+    cudaEvent_t fin;
+    if (cudaEventCreateWithFlags(&fin, cudaEventDisableTiming) == cudaSuccess) {
+        cudaEventRecord(fin, cs.st);
+        cudaStreamWaitEvent(os.st, fin, 0);
+        cudaEventDestroy(fin);
+    } else {
+        cudaStreamSynchronize(cs.st);
+    }
+    for (int i = 0; i < chunks; i++) cudaEventDestroy(cc.ev[i]);
+    if (le != cudaSuccess) return fail(DOL_ERR_CUDA, "launch failed: %s", cudaGetErrorString(le));
+    if (cc.err != cudaSuccess) return fail(DOL_ERR_CUDA, "copy to host failed: %s", cudaGetErrorString(cc.err));
+    const dol_status s1 = dol_sync(cs.st);
+    const dol_status s0 = dol_sync(os.st);
+    return s0 != DOL_OK ? s0 : s1;
 }
 
 }  // extern "C"

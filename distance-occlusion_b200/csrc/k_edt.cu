@@ -247,13 +247,13 @@ __device__ __forceinline__ void put_line_value(void* out, long long o, uint32_t 
 // it fits (kStaged) or read from global memory otherwise.
 template <typename TIn, bool kFinal, bool kStaged>
 __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, void* __restrict__ out, int w, int n,
-                                                  long long stride, long long outer_stride, int form)
+                                                  long long stride, long long outer_stride, int form, int outer0)
 {
     extern __shared__ unsigned char smem_raw[];
     TIn* tile = reinterpret_cast<TIn*>(smem_raw);   // [n][32]
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int x = blockIdx.x * 32 + lane;
-    const long long base = (long long)blockIdx.y * outer_stride + x;
+    const long long base = (long long)(blockIdx.y + outer0) * outer_stride + x;
     const bool live = x < w;
 
     if (kStaged) {
@@ -291,7 +291,7 @@ __device__ __forceinline__ uint32_t add_sq(TIn v, uint32_t k2)
 template <typename TIn, bool kFinal, int TX>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
-                                                      int along_z, int form, int* err)
+                                                      int along_z, int form, int* err, int outer0)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     TIn* F1 = F0 + rows * TX;                      // [rows][TX]
     __shared__ __align__(8) uint64_t bar;
     const int x0 = blockIdx.x * TX;
-    const int outer = blockIdx.y;
+    const int outer = blockIdx.y + outer0;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
 
 template <typename TIn, bool kFinal>
 static void line_pass_plain(const TIn* in, void* out, int w, int n, long long stride, long long outer,
-                            long long outer_stride, int form, cudaStream_t st)
+                            long long outer_stride, int form, cudaStream_t st, int outer0 = 0)
 {
     size_t bytes = (size_t)n * 32 * sizeof(TIn);
     const size_t kStageLimit = 200 * 1024;
@@ -393,22 +393,24 @@ static void line_pass_plain(const TIn* in, void* out, int w, int n, long long st
     if (bytes <= kStageLimit) {
         auto kern = k_edt_line<TIn, kFinal, true>;
         if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        kern<<<grid, 256, bytes, st>>>(in, out, w, n, stride, outer_stride, form);
+        kern<<<grid, 256, bytes, st>>>(in, out, w, n, stride, outer_stride, form, outer0);
     } else {
-        k_edt_line<TIn, kFinal, false><<<grid, 256, 0, st>>>(in, out, w, n, stride, outer_stride, form);
+        k_edt_line<TIn, kFinal, false><<<grid, 256, 0, st>>>(in, out, w, n, stride, outer_stride, form, outer0);
     }
 }
 
 // Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
-// of a w x h x d array.  TMA needs 16-byte row pitches and a tile that fits in
-// shared memory; otherwise the plain form runs.
+// of a w x h x d array; outer indices outer0 .. outer0 + nouter - 1 (nouter < 0:
+// all).  TMA needs 16-byte row pitches and a tile that fits in shared memory;
+// otherwise the plain form runs.
 template <typename TIn, bool kFinal>
-static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z, int form, int* err, cudaStream_t st)
+static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z, int form, int* err, cudaStream_t st,
+                      int outer0 = 0, int nouter = -1)
 {
     const int n = along_z ? d : h;
     const long long plane = (long long)w * h;
     const long long stride = along_z ? plane : w;
-    const long long outer = along_z ? h : d;
+    const long long outer = nouter >= 0 ? nouter : (along_z ? h : d);
     const long long outer_stride = along_z ? w : plane;
     constexpr int TX = sizeof(TIn) == 2 ? 16 : 8;   // 32-byte box rows either way
     const int nbox = (n + 255) / 256;
@@ -426,11 +428,11 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
             const int tv = tune_get(kTuneEdt, w);
             const int threads = tv == 256 ? 256 : 512;
-            kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err);
+            kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0);
             return;
         }
     }
-    line_pass_plain<TIn, kFinal>(in, out, w, n, stride, outer, outer_stride, form, st);
+    line_pass_plain<TIn, kFinal>(in, out, w, n, stride, outer, outer_stride, form, st, outer0);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -491,6 +493,31 @@ void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, in
         }
         ProfScope ps("edt_z_final", st);
         line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st);   // z lines
+    }
+}
+
+// The 3D mask EDT with the last (z) pass cut into `chunks` launches over ranges
+// of y; after each launch `done(ctx, y0, y1)` runs on the host so the caller can
+// queue work on rows y0..y1-1 of every slice (a copy back to the host that
+// overlaps the remaining launches).
+void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
+                                cudaStream_t st, int chunks, void (*done)(void*, int, int), void* ctx)
+{
+    const long long rows = (long long)h * d;
+    const size_t cells = (size_t)w * rows;
+    uint16_t* vx = static_cast<uint16_t*>(ws);
+    const long long blocks = (rows * 32 + 255) / 256, cap = (long long)g_num_sms * 16;
+    k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask, vx, w, rows);
+    const size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
+    uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
+    line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st);
+    if (chunks < 1) chunks = 1;
+    if (chunks > h) chunks = h;
+    for (int c = 0; c < chunks; c++) {
+        const int y0 = (int)((long long)h * c / chunks), y1 = (int)((long long)h * (c + 1) / chunks);
+        if (y1 <= y0) continue;
+        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st, y0, y1 - y0);
+        if (done) done(ctx, y0, y1);
     }
 }
 

@@ -173,6 +173,20 @@ def test_chamfer_rejects_bad_widths(dol, cuda):
             dol.chamfer(t, (w, 3))
 
 
+@pytest.mark.parametrize("dims", [(24, 20, 16), (40, 70, 9), (33, 100, 20), (64, 130, 3)])
+def test_edt_mask_host_chunked(dol, O, cuda, dims):
+    """dol_edt_mask_3d_host: host buffers, the last pass in y chunks with the copy
+    back overlapping it; same floats as the oracle in every form."""
+    rng = np.random.default_rng(sum(dims) + 3)
+    big = np.float32(np.finfo(np.float32).max)
+    for p in (0.0, 0.02, 0.4, 1.0):
+        m = rand_mask(O, rng, dims, p)
+        b = O.mask_to_bool(m, dims)
+        want_sq = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims)
+        same_float(dol.edt_mask_host(m, dims, dol.EDT_SQUARED), want_sq)
+        same_float(dol.edt_mask_host(m, dims, dol.EDT_SIGNED), O.sdf_signed_felzenszwalb(m, dims))
+
+
 @pytest.mark.parametrize("dims", [(8, 1000, 3), (16, 300, 37), (24, 5, 777), (8, 2049, 2), (40, 3, 1029),
                                   (2000, 8), (64, 1027)])
 def test_edt_mask_long_lines(dol, O, cuda, dims):

@@ -748,24 +748,35 @@ dol_status dol_batch_prepare(int n, const dol_batch_item* items, void* workspace
         if (it.w > 1024) return fail(DOL_ERR_UNSUPPORTED, "item %d: batched rows are limited to 1024 cells", i);
         if (it.mask_word_offset < 0 || it.delta_byte_offset < 0)
             return fail(DOL_ERR_INVALID_ARG, "item %d has a negative offset", i);
+        // 2D cells are read and written as 4-byte words, 3D cells as 2-byte halves
+        if (it.delta_byte_offset % (it.d > 1 ? 2 : 4) != 0)
+            return fail(DOL_ERR_INVALID_ARG, "item %d: delta_byte_offset %lld is not a multiple of %d bytes", i,
+                        it.delta_byte_offset, it.d > 1 ? 2 : 4);
         // serial row steps dominate: 2h per image, 2(d-1)*2h per volume, plus the cells themselves
         work[i] = it.d > 1 ? 4.0 * it.d * it.h + 1e-3 * it.w * it.h * it.d : 2.0 * it.h + 1e-3 * it.w * it.h;
         order[i] = i;
     }
-    // whole-CTA items first (volumes, then images with rows over 256 cells),
-    // then the one-warp images; each group by decreasing work
-    auto group = [&](int i) { return items[i].d > 1 ? 0 : (items[i].w > 256 ? 1 : 2); };
+    // queue A: volumes with rows of at most 256 cells (one warp each); queue B:
+    // items with wider rows (one CTA each), then the narrow images; each group
+    // by decreasing work
+    auto group = [&](int i) { return items[i].w > 256 ? 1 : (items[i].d > 1 ? 0 : 2); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         const int ga = group(a), gb = group(b);
         if (ga != gb) return ga < gb;
         return work[a] > work[b];
     });
+    int nv = 0;
+    for (int i = 0; i < n; i++) nv += group(i) == 0;
     char* p = static_cast<char*>(workspace);
     cudaStream_t st = S(stream);
     cudaError_t e = cudaMemcpyAsync(p, items, (size_t)n * sizeof(dol_batch_item), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p + align256((size_t)n * sizeof(dol_batch_item)), order.data(), (size_t)n * sizeof(int),
                             cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p + align256((size_t)n * sizeof(dol_batch_item)) + align256((size_t)n * sizeof(int)) +
+                                2 * sizeof(int),
+                            &nv, sizeof(int), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host order vector ends here
     if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "batch upload: %s", cudaGetErrorString(e));
     return DOL_OK;
@@ -776,6 +787,8 @@ dol_status dol_batch_run(int n, const uint32_t* masks, void* deltas, float* dist
     DeviceState* ds;
     DOL_TRY(device_state(&ds));
     if (n < 1 || !masks || !deltas || !workspace) return fail(DOL_ERR_INVALID_ARG, "missing batch buffer");
+    if (((uintptr_t)masks | (uintptr_t)deltas | (uintptr_t)dist) % 4 != 0)
+        return fail(DOL_ERR_INVALID_ARG, "batch buffers must be 4-byte aligned");
     char* p = static_cast<char*>(workspace);
     const void* items = p;
     const int* order = reinterpret_cast<const int*>(p + align256((size_t)n * sizeof(dol_batch_item)));

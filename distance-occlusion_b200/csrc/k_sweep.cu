@@ -845,11 +845,16 @@ __device__ __noinline__ void batch_item_warp(const BatchItemDev& b, const uint32
     }
 }
 
-// Items are ordered volumes first (their serial chains are the longest), then
-// wide images (rows > 256 cells), each by decreasing work, then the narrow
-// images: all of these but the narrow images take a whole CTA each.  The first
-// narrow image a CTA draws switches it to per-warp draining: each warp takes
-// narrow images on its own until the queue is empty.
+// Two queues.  Queue A (order[0 .. nv)) holds the volumes whose rows fit one
+// warp (up to 256 cells), longest chain first; queue B (order[nv .. n)) the
+// items with rows over 256 cells, then the narrow images.  A CTA takes queue A
+// items while there are any: the whole CTA runs the volume's border init and
+// its distances, while warp 0 alone runs the serial sweep with the
+// single-warp engine (no CTA barriers in the chain; 1.5-2x faster than the
+// CTA engine on rows this narrow).  Then it turns to queue B: items with wide
+// rows take the whole CTA; the first narrow image it draws switches it to
+// per-warp draining.  counter: [0] queue B, [1] queue A, [2] nv (written by
+// dol_batch_prepare).
 template <int S>
 __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restrict__ items, const int* __restrict__ order,
                                                    int n, const uint32_t* __restrict__ masks,
@@ -860,20 +865,41 @@ __global__ void __launch_bounds__(256) k_batch_sdf(const BatchItemDev* __restric
     __shared__ int s_item;
     ScanShared<C2>& sh2 = *reinterpret_cast<ScanShared<C2>*>(&sh3);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nv = counter[2];
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) s_item = atomicAdd(counter + 1, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= nv) break;
+        const BatchItemDev b = items[order[it]];
+        const uint32_t* m = masks + b.mask_off;
+        int16_t* dl = reinterpret_cast<int16_t*>(deltas + b.delta_off);
+        border3_cta(m, dl, b.w, b.h, b.d);
+        __syncthreads();
+        if (warp == 0) {
+            if (b.w <= 64) danielsson3_warp<2>(dl, b.w, b.h, b.d, 2);
+            else if (b.w <= 128) danielsson3_warp<4>(dl, b.w, b.h, b.d, 2);
+            else danielsson3_warp<8>(dl, b.w, b.h, b.d, 2);
+        }
+        __syncthreads();
+        if (dist && b.dist_off >= 0) signed_dist_cta<C3>(m, dl, dist + b.dist_off, b.w, (long long)b.h * b.d);
+        __syncthreads();
+    }
+    for (;;) {
+        if (threadIdx.x == 0) s_item = nv + atomicAdd(counter, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();
         if (it >= n) return;
         const BatchItemDev b = items[order[it]];
-        if (b.d <= 1 && b.w <= 256) {
+        if (b.w <= 256) {
             // narrow images from here on: warp 0 takes this item, every warp then drains the queue
             int mine = warp == 0 ? it : -1;
             for (;;) {
                 if (mine < 0) {
                     int v = 0;
-                    if (lane == 0) v = atomicAdd(counter, 1);
+                    if (lane == 0) v = nv + atomicAdd(counter, 1);
                     mine = __shfl_sync(0xFFFFFFFFu, v, 0);
                     if (mine >= n) return;
                 }
@@ -919,7 +945,7 @@ void launch_batch_sdf(const void* items, const int* order, int n, const uint32_t
     int grid = per_sm * g_num_sms;
     if (grid > n) grid = n;
     if (grid < 1) grid = 1;
-    cudaMemsetAsync(counter, 0, sizeof(int), st);
+    cudaMemsetAsync(counter, 0, 2 * sizeof(int), st);   // the queue heads; counter[2] (nv) stays
     if (eight)
         k_batch_sdf<8><<<grid, threads, 0, st>>>(static_cast<const BatchItemDev*>(items), order, n, masks,
                                                  static_cast<unsigned char*>(deltas), dist, counter);

@@ -162,6 +162,22 @@ def sdf_two_pass(mask, dims, method, use_ref=False):
     return d0, d1, dist
 
 
+# ---- accuracy against BruteForce ----------------------------------------------------------
+
+ERR_EDGES = np.array([0.0, 1e-6, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.75, 1.0, np.inf], dtype=np.float64)
+
+
+def error_histogram(deltas, refs, dims, edges=ERR_EDGES):
+    """The tool's error measure (PrintError, DistanceOcclusionTool.cpp:265-287): per cell
+    |Dist(delta) - Dist(ref)| in float, Dist = sqrtf of the int32 squared length (:46-61).
+    Returns (counts per [edges[i], edges[i+1]), max error)."""
+    a = deltas_to_dist(np.ascontiguousarray(deltas), dims, 1)
+    b = deltas_to_dist(np.ascontiguousarray(refs), dims, 1)
+    err = np.abs(a - b).astype(np.float32)
+    counts, _ = np.histogram(err.astype(np.float64), bins=edges)
+    return counts, float(err.max()) if err.size else 0.0
+
+
 # ---- Chamfer (integer distances) ----------------------------------------------------------
 
 def init_distances_int(mask, dims, dtype, max_d, use_ref=False):

@@ -87,6 +87,24 @@ def test_config1_against_reference_digests(dol, O, cuda, dims):
     assert hashlib.sha256(sq.tobytes()).hexdigest() == dig["c1_felz"]
 
 
+def test_config1_error_histogram_vs_bruteforce(dol, O, cuda):
+    """The 1024^2 image with 100 points (seed 1): the GPU Danielsson's error
+    histogram against BruteForce (the tool's PrintError measure) equals the
+    reference CPU Danielsson's, and its maximum error is below one cell (the
+    tool's pass criterion)."""
+    dims = (1024, 1024)
+    m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+    ini = O.init_deltas(m, dims)
+    got = host(dol.propagate("danielsson", dol.init_deltas(dev(cuda, m), dims), dims, 1))
+    bf = O.propagate("bruteforce", ini, dims, 1)
+    want = O.propagate("danielsson", ini, dims, 1)
+    h_gpu, max_gpu = O.error_histogram(got, bf, dims)
+    h_cpu, max_cpu = O.error_histogram(want, bf, dims)
+    np.testing.assert_array_equal(h_gpu, h_cpu)
+    assert max_gpu == max_cpu < 1.0
+    assert h_gpu.sum() == dims[0] * dims[1]
+
+
 def test_volume64_against_reference_digests(dol, O, cuda):
     with open(os.path.join(HERE, "golden", "golden_digests.json")) as f:
         dig = json.load(f)

@@ -110,6 +110,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x, pg, device="cuda"):
+    """The slowest rank's value; every rank calls it (a no-op on one rank)."""
+    if not pg:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gvox_per_s(world, voxels_per_rank, seconds):
+    """Whole-job throughput of `world` independent replicas timed at `seconds` (max over ranks)."""
+    return world * voxels_per_rank / seconds / 1e9
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -545,12 +560,9 @@ def run_dol(args):
     if pg:
         pg.barrier()
     clk = clocks.stop()
-    if pg:
-        t = torch.tensor([ms_total], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, pg)
     ms_step = ms_total / args.steps
-    value = ws * W * H * D / (ms_step * 1e-3) / 1e9
+    value = job_gvox_per_s(ws, W * H * D, ms_step * 1e-3)
 
     # e2e: host mask in (pinned), host field out (pinned), through the host-buffer C ABI call
     e2e = None
@@ -566,12 +578,8 @@ def run_dol(args):
                                              C.c_void_p(hout.data_ptr()), C.c_int(dol.EDT_SIGNED)))
             if i >= args.e2e_warmup:
                 ts.append(time.perf_counter() - t)
-        e2e_s = float(np.mean(ts))
-        if pg:
-            t = torch.tensor([e2e_s], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": ws * W * H * D / e2e_s / 1e9, "unit": "Gvoxels/s", "h2d_bytes_per_step": mw * 4,
+        e2e_s = max_over_ranks(float(np.mean(ts)), pg)
+        e2e = {"value": job_gvox_per_s(ws, W * H * D, e2e_s), "unit": "Gvoxels/s", "h2d_bytes_per_step": mw * 4,
                "d2h_bytes_per_step": W * H * D * 4, "ms_per_step": e2e_s * 1e3,
                "path": "dol_edt_mask_3d_host, pinned host buffers"}
 

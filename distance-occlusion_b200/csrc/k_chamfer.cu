@@ -14,10 +14,12 @@
 // sums do not wrap (every input at most INT32_MAX - 4).  The way up mirrors it
 // (suffix min, right neighbour).
 //
-// One CTA per field walks the rows (each row needs the one before); a thread
-// owns 4 consecutive cells, so rows of up to 4096 cells.  The previous row
-// sits in shared memory with "no value" sentinels at x = -1 and x = w; two
-// barriers per row (warp totals, the next row's neighbours).
+// A CTA walks a run of rows (each row needs the one before); a thread owns 4
+// consecutive cells, so rows of up to 4096 cells.  The previous row sits in
+// shared memory with "no value" sentinels at x = -1 and x = w; two barriers
+// per row (warp totals, the next row's neighbours).  Fields of 64 rows or more
+// run in blocks of 32 rows, all blocks at once (see below); smaller ones, or
+// when the small boundary scratch cannot be had, in one CTA.
 #include <type_traits>
 
 #include "common.cuh"
@@ -79,13 +81,14 @@ __device__ __forceinline__ K block_excl_min(K tot, K* wtot, K inf)
     return min(excl, mine);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(1024) k_chamfer2(T* __restrict__ dist, int w, int h)
+// Rows ya, ya + dir, ..., yb of one pass (dir = +1 down, -1 up), the first of
+// them with no row before it; one CTA, a thread per 4 consecutive cells.
+template <typename T, bool kFwd>
+__device__ __forceinline__ void chamfer_rows(T* __restrict__ dist, int w, int ya, int yb, unsigned char* smem_raw)
 {
     using K = typename ChamferKey<T>::K;
     constexpr K kInf = ChamferKey<T>::kInf;
     constexpr int C = kChamferCells;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     K* prev = reinterpret_cast<K*>(smem_raw);   // [2][w + 2], cell x at index x + 1
     K* wtot = prev + 2 * (w + 2);               // [32]
     const int x0 = threadIdx.x * C;
@@ -93,23 +96,18 @@ __global__ void __launch_bounds__(1024) k_chamfer2(T* __restrict__ dist, int w, 
         prev[0] = prev[w + 1] = kInf;
         prev[w + 2] = prev[2 * (w + 2) - 1] = kInf;
     }
-
-    K v[C], r[C];
-    auto load_row = [&](int y) {
-#pragma unroll
-        for (int c = 0; c < C; c++) v[c] = x0 + c < w ? (K)dist[(long long)y * w + x0 + c] : kInf;
-    };
-    // one row: u from v and the previous row (if any), then the min-plus scan along dir
-    auto row = [&](auto fwd_tag, int y, const K* pv, K* pn) {
-        constexpr bool kFwd = decltype(fwd_tag)::value;
+    __syncthreads();
+    int b = 0;
+    const int dir = kFwd ? 1 : -1;
+    for (int y = ya;; y += dir) {
+        const K* pv = y == ya ? nullptr : prev + b * (w + 2);
+        K* pn = prev + (b ^ 1) * (w + 2);
         K u[C];
 #pragma unroll
         for (int c = 0; c < C; c++) {
-            u[c] = v[c];
-            if (pv && x0 + c < w) {
-                const int i = x0 + c + 1;
-                u[c] = min(u[c], min(min(pv[i - 1], pv[i + 1]) + 4, pv[i] + 3));
-            }
+            const int x = x0 + c;
+            u[c] = x < w ? (K)dist[(long long)y * w + x] : kInf;
+            if (pv && x < w) u[c] = min(u[c], min(min(pv[x], pv[x + 2]) + 4, pv[x + 1] + 3));
         }
         K m[C];
         if (kFwd) {
@@ -129,37 +127,149 @@ __global__ void __launch_bounds__(1024) k_chamfer2(T* __restrict__ dist, int w, 
 #pragma unroll
         for (int c = 0; c < C; c++) {
             const int x = x0 + c;
-            r[c] = kFwd ? min(ex, m[c]) + 3 * (K)x : min(ex, m[c]) - 3 * (K)x;
+            const K r = kFwd ? min(ex, m[c]) + 3 * (K)x : min(ex, m[c]) - 3 * (K)x;
             if (x < w) {
-                dist[(long long)y * w + x] = (T)r[c];
-                pn[x + 1] = r[c];
+                dist[(long long)y * w + x] = (T)r;
+                pn[x + 1] = r;
             }
         }
         __syncthreads();   // the next row reads pn; the next scan rewrites wtot
-    };
-    using Fwd = std::true_type;
-    using Bwd = std::false_type;
+        b ^= 1;
+        if (y == yb) break;
+    }
+}
 
-    __syncthreads();
-    // down the rows
-    int b = 0;
-    load_row(0);
-    row(Fwd{}, 0, (const K*)nullptr, prev + b * (w + 2));
-    for (int y = 1; y < h; y++) {
-        load_row(y);
-        row(Fwd{}, y, prev + b * (w + 2), prev + (b ^ 1) * (w + 2));
-        b ^= 1;
+// the whole field in one CTA: down the rows, then back up
+template <typename T>
+__global__ void __launch_bounds__(1024) k_chamfer2(T* __restrict__ dist, int w, int h)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    chamfer_rows<T, true>(dist, w, 0, h - 1, smem_raw);
+    chamfer_rows<T, false>(dist, w, h - 1, 0, smem_raw);
+}
+
+// ---- the same passes over blocks of R rows ----
+// A pass only takes mins of sums of exact integers, so it is min-plus linear:
+// a block's result is the min of (a) the block run with nothing before its
+// first row and (b) the boundary row before it carried through the block with
+// every cell of the block "no value".  (b) has a closed form: a cell r rows
+// past the boundary row gets min over j of T[j] + c(x - j, r), c the cheapest
+// path of the pass's steps (3 straight, 4 diagonal, along the row only in the
+// scan direction): c = 3 max(|dx|, r) + min(|dx|, r) where the path can reach,
+// i.e. |dx| <= r, or any dx on the side the row scan moves towards.  So:
+//   1. every block runs with nothing before it (parallel over blocks);
+//   2. one CTA walks the blocks: a block's true last row is the min of its
+//      row from step 1 and the previous true last row carried R rows;
+//   3. every row of every block takes the min with the previous block's true
+//      last row carried to it (parallel over rows).
+constexpr int kChamferBlockRows = 32;
+
+template <typename T, bool kFwd>
+__global__ void __launch_bounds__(1024) k_chamfer_blocks(T* __restrict__ dist, int w, int h, int R)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int y0 = blockIdx.x * R, y1 = min(h, y0 + R);
+    if (kFwd)
+        chamfer_rows<T, true>(dist, w, y0, y1 - 1, smem_raw);
+    else
+        chamfer_rows<T, false>(dist, w, y1 - 1, y0, smem_raw);
+}
+
+// The boundary row bt carried r rows into the next block, at cell x: the window
+// |x - j| <= r (cost 3r + |x - j|) and the far side the scan moves from (pre:
+// prefix min of bt[j] - 3j going down, suffix min of bt[j] + 3j going up).
+template <typename K, bool kFwd>
+__device__ __forceinline__ K carried(const K* bt, const K* pre, int w, int x, int r, K inf)
+{
+    K best = inf;
+    const int ja = max(0, x - r), jb = min(w - 1, x + r);
+    for (int j = ja; j <= jb; j++) best = min(best, bt[j] + 3 * (K)r + (K)abs(x - j));
+    if (kFwd) {
+        if (x - r - 1 >= 0) best = min(best, pre[x - r - 1] + 3 * (K)x + (K)r);
+    } else {
+        if (x + r + 1 < w) best = min(best, pre[x + r + 1] - 3 * (K)x + (K)r);
     }
-    // back up: the last row starts from its result on the way down
+    return best;
+}
+
+// Step 2: one CTA walks the blocks in scan order and keeps each true boundary
+// row (bt[blk]) with its prefix / suffix minima (pre[blk]) for step 3.
+template <typename T, bool kFwd>
+__global__ void __launch_bounds__(1024) k_chamfer_chain(T* __restrict__ dist, int w, int h, int R,
+                                                        typename ChamferKey<T>::K* __restrict__ bt,
+                                                        typename ChamferKey<T>::K* __restrict__ pre)
+{
+    using K = typename ChamferKey<T>::K;
+    constexpr K kInf = ChamferKey<T>::kInf;
+    constexpr int C = kChamferCells;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* cur = reinterpret_cast<K*>(smem_raw);   // [w] boundary row
+    K* cpre = cur + w;                          // [w] its prefix / suffix minima
+    K* wtot = cpre + w;                         // [32]
+    const int nb = (h + R - 1) / R;
+    const int x0 = threadIdx.x * C;
+    for (int s = 0; s < nb - 1; s++) {
+        const int blk = kFwd ? s : nb - 1 - s;          // the block whose boundary row this is
+        const int yb = kFwd ? min(h, (blk + 1) * R) - 1 : blk * R;   // its last row in scan order
+        K v[C];
 #pragma unroll
-    for (int c = 0; c < C; c++) v[c] = x0 + c < w ? r[c] : kInf;
-    row(Bwd{}, h - 1, (const K*)nullptr, prev + (b ^ 1) * (w + 2));
-    b ^= 1;
-    for (int y = h - 2; y >= 0; y--) {
-        load_row(y);
-        row(Bwd{}, y, prev + b * (w + 2), prev + (b ^ 1) * (w + 2));
-        b ^= 1;
+        for (int c = 0; c < C; c++) {
+            const int x = x0 + c;
+            v[c] = x < w ? (K)dist[(long long)yb * w + x] : kInf;
+            if (s > 0 && x < w) {
+                const int rows = kFwd ? yb - (blk * R - 1) : (blk + 1) * R - yb;
+                v[c] = min(v[c], carried<K, kFwd>(cur, cpre, w, x, rows, kInf));
+            }
+        }
+        __syncthreads();   // every thread has read the previous boundary row
+        K m[C];
+        if (kFwd) {
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                const K key = x0 + c < w ? v[c] - 3 * (K)(x0 + c) : kInf;
+                m[c] = c ? min(m[c - 1], key) : key;
+            }
+        } else {
+#pragma unroll
+            for (int c = C - 1; c >= 0; c--) {
+                const K key = x0 + c < w ? v[c] + 3 * (K)(x0 + c) : kInf;
+                m[c] = c < C - 1 ? min(m[c + 1], key) : key;
+            }
+        }
+        const K ex = block_excl_min<K, kFwd>(kFwd ? m[C - 1] : m[0], wtot, kInf);
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const int x = x0 + c;
+            if (x < w) {
+                const K pm = min(ex, m[c]);
+                cur[x] = v[c];
+                cpre[x] = pm;
+                bt[(long long)blk * w + x] = v[c];
+                pre[(long long)blk * w + x] = pm;
+            }
+        }
+        __syncthreads();
     }
+}
+
+// Step 3: every row of a block after the first in scan order takes the min with
+// the previous block's true boundary row carried to it.
+template <typename T, bool kFwd>
+__global__ void __launch_bounds__(256) k_chamfer_apply(T* __restrict__ dist, int w, int h, int R,
+                                                       const typename ChamferKey<T>::K* __restrict__ bt,
+                                                       const typename ChamferKey<T>::K* __restrict__ pre)
+{
+    using K = typename ChamferKey<T>::K;
+    constexpr K kInf = ChamferKey<T>::kInf;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int blk = y / R, nb = (h + R - 1) / R;
+    if (x >= w || (kFwd ? blk == 0 : blk == nb - 1)) return;
+    const int src = kFwd ? blk - 1 : blk + 1;
+    const int rows = kFwd ? y - (blk * R - 1) : (blk + 1) * R - y;
+    const K c = carried<K, kFwd>(bt + (long long)src * w, pre + (long long)src * w, w, x, rows, kInf);
+    T* p = dist + (long long)y * w + x;
+    if (c < (K)*p) *p = (T)c;
 }
 
 template <typename T>
@@ -186,9 +296,35 @@ void launch_chamfer_2d(T* dist, int w, int h, cudaStream_t st)
 {
     using K = typename ChamferKey<T>::K;
     const size_t smem = (2 * (size_t)(w + 2) + 32) * sizeof(K);
+    const int threads = chamfer_threads(w);
     ProfScope ps("chamfer_2d", st);
+    const int R = kChamferBlockRows, nb = (h + R - 1) / R;
+    void* scratch = nullptr;
+    const size_t sb = 2 * (size_t)nb * w * sizeof(K);
+    if (nb >= 2 && h <= 65535 && cudaMallocAsync(&scratch, sb, st) == cudaSuccess) {
+        K* bt = static_cast<K*>(scratch);
+        K* pre = bt + (size_t)nb * w;
+        const size_t csmem = (2 * (size_t)w + 32) * sizeof(K);
+        auto set = [](const void* f, size_t b) {
+            if (b > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+        };
+        set((const void*)k_chamfer_blocks<T, true>, smem);
+        set((const void*)k_chamfer_blocks<T, false>, smem);
+        set((const void*)k_chamfer_chain<T, true>, csmem);
+        set((const void*)k_chamfer_chain<T, false>, csmem);
+        const dim3 ag((w + 255) / 256, h);
+        k_chamfer_blocks<T, true><<<nb, threads, smem, st>>>(dist, w, h, R);
+        k_chamfer_chain<T, true><<<1, threads, csmem, st>>>(dist, w, h, R, bt, pre);
+        k_chamfer_apply<T, true><<<ag, 256, 0, st>>>(dist, w, h, R, bt, pre);
+        k_chamfer_blocks<T, false><<<nb, threads, smem, st>>>(dist, w, h, R);
+        k_chamfer_chain<T, false><<<1, threads, csmem, st>>>(dist, w, h, R, bt, pre);
+        k_chamfer_apply<T, false><<<ag, 256, 0, st>>>(dist, w, h, R, bt, pre);
+        cudaFreeAsync(scratch, st);
+        return;
+    }
+    cudaGetLastError();   // a failed scratch allocation: walk the whole field in one CTA
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_chamfer2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_chamfer2<T><<<1, chamfer_threads(w), smem, st>>>(dist, w, h);
+    k_chamfer2<T><<<1, threads, smem, st>>>(dist, w, h);
 }
 
 template <typename T>

@@ -156,7 +156,7 @@ def test_sdf_two_pass(dol, O, cuda, dims, method):
 
 
 @pytest.mark.parametrize("dims", [(2, 1), (2, 9), (3, 1), (31, 7), (64, 64), (100, 37), (257, 19), (1000, 5),
-                                  (4096, 3), (33, 300)])
+                                  (4096, 3), (33, 300), (2, 100), (5, 2000), (100, 129), (300, 257), (1024, 1024)])
 def test_chamfer(dol, O, cuda, dims):
     """Chamfer 3-4 on int16 and int32 fields against the oracle, bit for bit: the
     tool's init (INT16_MAX - 16), masks of every density, and arbitrary values

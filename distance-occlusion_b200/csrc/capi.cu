@@ -461,8 +461,8 @@ dol_status dol_fastsweep_3d(int w, int h, int d, dol_delta3* deltas, int cw, voi
     return launched("fastsweep_3d");
 }
 
-size_t dol_jumpflood_2d_workspace_size(int w, int h) { return (size_t)w * h * sizeof(dol_delta2); }
-size_t dol_jumpflood_3d_workspace_size(int w, int h, int d) { return (size_t)w * h * d * sizeof(dol_delta3); }
+size_t dol_jumpflood_2d_workspace_size(int w, int h) { return jumpflood_workspace_bytes(2, w, h, 1); }
+size_t dol_jumpflood_3d_workspace_size(int w, int h, int d) { return jumpflood_workspace_bytes(3, w, h, d); }
 
 dol_status dol_jumpflood_2d(int w, int h, dol_delta2* deltas, int cw, void* workspace, size_t workspace_bytes,
                             void* stream)
@@ -583,7 +583,7 @@ size_t dol_sdf_workspace_size(int w, int h, int d, int method)
     const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
     if (method == DOL_FELZENSZWALB) return edt_workspace_bytes(dim, w, h, d);
     size_t b = align256(cells * cb);                       // deltas, when the caller passes none
-    if (method == DOL_JUMPFLOOD) b += align256(cells * cb);  // ping-pong buffer
+    if (method == DOL_JUMPFLOOD) b += align256(jumpflood_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
     if (method == DOL_FASTSWEEP && dim == 3) b += align256(fastsweep3_workspace_bytes(w, h, d));
     if (method == DOL_DANIELSSON) b += align256(danielsson_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
     return b;
@@ -657,7 +657,7 @@ size_t dol_sdf_two_pass_workspace_size(int w, int h, int d, int method)
     const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
     const size_t cb = dim == 3 ? sizeof(dol_delta3) : sizeof(dol_delta2);
     size_t b = 2 * align256(cells * cb);                    // exterior / interior deltas the caller does not keep
-    if (method == DOL_JUMPFLOOD) b += align256(cells * cb);  // ping-pong buffer
+    if (method == DOL_JUMPFLOOD) b += align256(jumpflood_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
     if (method == DOL_FASTSWEEP && dim == 3) b += align256(fastsweep3_workspace_bytes(w, h, d));
     if (method == DOL_DANIELSSON) b += align256(danielsson_workspace_bytes(dim, w, h, dim == 3 ? d : 1));
     return b;

@@ -48,9 +48,22 @@ __device__ __forceinline__ void store3(int16_t* p, long long i, C3 v)
     c[1] = (int16_t)v.y;
     c[2] = (int16_t)v.z;
 }
+// Between its first and last pass the 3D JumpFlood keeps cells in 8 bytes
+// (x, y, z, unused): one aligned load per neighbour instead of three.
+__device__ __forceinline__ C3 load3w(const uint2* p, long long i)
+{
+    const uint2 u = __ldg(p + i);
+    return C3{(int)(int16_t)(u.x & 0xFFFFu), (int)(int16_t)(u.x >> 16), (int)(int16_t)(u.y & 0xFFFFu)};
+}
+__device__ __forceinline__ void store3w(uint2* p, long long i, C3 v)
+{
+    p[i] = make_uint2((uint32_t)(uint16_t)v.x | ((uint32_t)(uint16_t)v.y << 16), (uint32_t)(uint16_t)v.z);
+}
 
-__global__ void __launch_bounds__(512) k_jfa3(const int16_t* __restrict__ in, int16_t* __restrict__ out, int w, int h,
-                                              int d, int s, int cw)
+// kWideIn / kWideOut: 8-byte cells (the ping-pong buffers) or the caller's 6-byte cells
+template <bool kWideIn, bool kWideOut>
+__global__ void __launch_bounds__(512) k_jfa3(const void* __restrict__ in, void* __restrict__ out, int w, int h, int d,
+                                              int s, int cw)
 {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31);
     const int y = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -58,7 +71,10 @@ __global__ void __launch_bounds__(512) k_jfa3(const int16_t* __restrict__ in, in
     if (x >= w || y >= h) return;
     const long long plane = (long long)w * h;
     const long long idx = z * plane + (long long)y * w + x;
-    C3 best = load3(in, idx);
+    auto ld = [&](long long i) -> C3 {
+        return kWideIn ? load3w(static_cast<const uint2*>(in), i) : load3(static_cast<const int16_t*>(in), i);
+    };
+    C3 best = ld(idx);
     // all offsets in {-s, 0, +s}^3 that stay inside, z outermost, x innermost,
     // skipping neighbours still at max (:2419-2438)
     const int z0 = z - s >= 0 ? -s : 0, z1 = z + s < d ? s : 0;
@@ -67,11 +83,21 @@ __global__ void __launch_bounds__(512) k_jfa3(const int16_t* __restrict__ in, in
     for (int kz = z0; kz <= z1; kz += s)
         for (int ky = y0; ky <= y1; ky += s)
             for (int kx = x0; kx <= x1; kx += s) {
-                C3 c = load3(in, idx + kz * plane + (long long)ky * w + kx);
+                C3 c = ld(idx + kz * plane + (long long)ky * w + kx);
                 if (c.x == kMax3) continue;
                 best = closer(best, add(c, cw * kx, cw * ky, cw * kz));
             }
-    store3(out, idx, best);
+    if (kWideOut)
+        store3w(static_cast<uint2*>(out), idx, best);
+    else
+        store3(static_cast<int16_t*>(out), idx, best);
+}
+
+size_t jumpflood_workspace_bytes(int dim, int w, int h, int d)
+{
+    const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
+    if (dim == 2) return cells * sizeof(uint32_t);
+    return 2 * (((cells * sizeof(uint2)) + 255) & ~(size_t)255);
 }
 
 static int floor_pow2(int v)
@@ -88,30 +114,45 @@ void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, in
 {
     int m = w > h ? w : h;
     if (dim == 3 && d > m) m = d;
-    void* a = deltas;
-    void* b = temp;
     // rows per CTA (32 x ry threads): tuned, else 8
     int ry = tune_get(dim == 2 ? kTuneJfa2 : kTuneJfa3, w);
     if (ry != 2 && ry != 4 && ry != 8 && ry != 16) ry = 8;
-    auto pass = [&](int s, const void* src, void* dst) {
-        ProfScope ps("jumpflood_pass", st);
-        if (dim == 2) {
-            dim3 grid((w + 31) / 32, (h + ry - 1) / ry);
-            k_jfa2<<<grid, 32 * ry, 0, st>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), w, h, s,
+    // the reference's schedule: steps FloorPow2(m - 1) .. 1 ping-ponging with
+    // the caller's buffer, plus one step-1 pass when the result would end in temp
+    int steps[40], np = 0;
+    for (int s = floor_pow2(m - 1); s > 0; s /= 2) steps[np++] = s;
+    if (np & 1) steps[np++] = 1;
+    if (dim == 2) {
+        void* a = deltas;
+        void* b = temp;
+        const dim3 grid((w + 31) / 32, (h + ry - 1) / ry);
+        for (int i = 0; i < np; i++) {
+            ProfScope ps("jumpflood_pass", st);
+            k_jfa2<<<grid, 32 * ry, 0, st>>>(static_cast<const uint32_t*>(a), static_cast<uint32_t*>(b), w, h, steps[i],
                                              cw);
-        } else {
-            dim3 grid((w + 31) / 32, (h + ry - 1) / ry, d);
-            k_jfa3<<<grid, 32 * ry, 0, st>>>(static_cast<const int16_t*>(src), static_cast<int16_t*>(dst), w, h, d, s,
-                                             cw);
+            void* t = a;
+            a = b;
+            b = t;
         }
-    };
-    for (int s = floor_pow2(m - 1); s > 0; s /= 2) {
-        pass(s, a, b);
-        void* t = a;
-        a = b;
-        b = t;
+        return;
     }
-    if (a != deltas) pass(1, a, deltas);
+    // 3D: the caller's 6-byte cells -> 8-byte ping-pong buffers -> the caller's cells
+    const size_t cells = (size_t)w * h * d;
+    uint2* wb[2] = {static_cast<uint2*>(temp),
+                    reinterpret_cast<uint2*>(static_cast<char*>(temp) + (((cells * sizeof(uint2)) + 255) & ~(size_t)255))};
+    const dim3 grid((w + 31) / 32, (h + ry - 1) / ry, d);
+    for (int i = 0; i < np; i++) {
+        ProfScope ps("jumpflood_pass", st);
+        const bool first = i == 0, last = i == np - 1;
+        const void* src = first ? deltas : wb[(i - 1) & 1];
+        void* dst = last ? deltas : wb[i & 1];
+        if (first)
+            k_jfa3<false, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+        else if (last)
+            k_jfa3<true, false><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+        else
+            k_jfa3<true, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+    }
 }
 
 // ---- deltas -> distances (DistanceOcclusionTool.cpp:46-61, sign :1262/:1392) ----

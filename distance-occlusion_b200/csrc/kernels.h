@@ -70,6 +70,8 @@ size_t felz_float_workspace_bytes(int w, int h);
 void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st);
 
 // k_jfa.cu
+// temp: jumpflood_workspace_bytes (3D: two 8-byte-cell ping-pong buffers)
+size_t jumpflood_workspace_bytes(int dim, int w, int h, int d);
 void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, int cw, cudaStream_t st);
 void launch_deltas_to_dist(int dim, const void* deltas, int cw, const uint32_t* sign_mask, float* out, int w, int h,
                            int d, cudaStream_t st);

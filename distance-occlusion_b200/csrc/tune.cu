@@ -193,7 +193,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
                                        : fastsweep3_workspace_bytes(tw, th, td);
     bool ok = cudaMallocAsync(&dm, mwords * 4, st) == cudaSuccess &&
               cudaMallocAsync(&dl, (size_t)cells * (kind == kTuneEdt ? 4 : cell_bytes), st) == cudaSuccess &&
-              cudaMallocAsync(&tmp, (size_t)cells * cell_bytes, st) == cudaSuccess &&
+              cudaMallocAsync(&tmp, jumpflood_workspace_bytes(vol ? 3 : 2, tw, th, td), st) == cudaSuccess &&
               cudaMallocAsync(&ws, ws_bytes, st) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();

@@ -123,8 +123,11 @@ DOL_API dol_status dol_fastsweep_2d(int w, int h, dol_delta2* deltas, int cw, vo
 DOL_API size_t     dol_fastsweep_3d_workspace_size(int w, int h, int d);
 DOL_API dol_status dol_fastsweep_3d(int w, int h, int d, dol_delta3* deltas, int cw,
                             void* workspace, size_t workspace_bytes, void* stream);
-/* JumpFlood (DistanceOcclusionLib.cpp:887-908, :2450-2472); the workspace is
-   the reference's internal ping-pong buffer (one cell per cell) */
+/* JumpFlood (DistanceOcclusionLib.cpp:887-908, :2450-2472); the workspace
+   stands for the reference's internal ping-pong buffer: one 4-byte cell per
+   cell in 2D; in 3D two buffers of 8-byte cells (one aligned load per
+   neighbour), the caller's 6-byte cells being read by the first pass and
+   written by the last */
 DOL_API size_t     dol_jumpflood_2d_workspace_size(int w, int h);
 DOL_API size_t     dol_jumpflood_3d_workspace_size(int w, int h, int d);
 DOL_API dol_status dol_jumpflood_2d(int w, int h, dol_delta2* deltas, int cw,

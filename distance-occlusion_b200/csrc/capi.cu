@@ -1001,32 +1001,52 @@ dol_status dol_sdf_3d_host(int w, int h, int d, const uint32_t* mask, int method
     return sdf_host(3, w, h, d, mask, method, deltas, dist);
 }
 
-// The z pass runs in y chunks; each chunk's rows go back to the host on a
-// second stream while the next chunk computes (cudaMemcpy2DAsync: the chunk's
-// rows of every slice, one slice pitch apart).
-struct ChunkCopy {
+// Host-buffer 3D EDT with the copies overlapped: the mask goes up in slabs of
+// slices on the copy-in stream, the x and y passes of a slab start when its
+// slices have arrived, and the z pass runs in chunks of y whose rows go back
+// to the host on two copy-out streams in turn (cudaMemcpy2DAsync: the chunk's
+// rows of every slice, one slice pitch apart) while the next chunk computes.
+constexpr int kHostSlabs = 8, kHostChunks = 16;
+struct HostCopies {
+    const uint32_t* hmask;
+    uint32_t* dmask;
     float* host;
     const float* dev;
     int w, h, d;
-    cudaStream_t compute, copy;
-    cudaEvent_t ev[16];
+    cudaStream_t compute, in, out[2];
+    cudaEvent_t ev[kHostSlabs + kHostChunks];
     int n;
     cudaError_t err;
 };
 
+static void slab_ready(void* ctx, int z0, int z1)
+{
+    HostCopies* hc = static_cast<HostCopies*>(ctx);
+    if (hc->err != cudaSuccess || hc->n >= kHostSlabs + kHostChunks) return;
+    const size_t words = (size_t)((hc->w + 31) / 32) * hc->h;   // mask words per slice
+    cudaEvent_t e = hc->ev[hc->n++];
+    cudaError_t r = cudaMemcpyAsync(hc->dmask + (size_t)z0 * words, hc->hmask + (size_t)z0 * words,
+                                    (size_t)(z1 - z0) * words * sizeof(uint32_t), cudaMemcpyHostToDevice, hc->in);
+    if (r == cudaSuccess) r = cudaEventRecord(e, hc->in);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(hc->compute, e, 0);
+    if (r != cudaSuccess) hc->err = r;
+}
+
 static void chunk_done(void* ctx, int y0, int y1)
 {
-    ChunkCopy* cc = static_cast<ChunkCopy*>(ctx);
-    if (cc->err != cudaSuccess || cc->n >= 16) return;
-    cudaEvent_t e = cc->ev[cc->n++];
-    const size_t pitch = (size_t)cc->w * cc->h * sizeof(float);
-    const size_t first = (size_t)y0 * cc->w;
-    cudaError_t r = cudaEventRecord(e, cc->compute);
-    if (r == cudaSuccess) r = cudaStreamWaitEvent(cc->copy, e, 0);
+    HostCopies* hc = static_cast<HostCopies*>(ctx);
+    if (hc->err != cudaSuccess || hc->n >= kHostSlabs + kHostChunks) return;
+    const int i = hc->n;
+    cudaEvent_t e = hc->ev[hc->n++];
+    cudaStream_t cs = hc->out[i & 1];
+    const size_t pitch = (size_t)hc->w * hc->h * sizeof(float);
+    const size_t first = (size_t)y0 * hc->w;
+    cudaError_t r = cudaEventRecord(e, hc->compute);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(cs, e, 0);
     if (r == cudaSuccess)
-        r = cudaMemcpy2DAsync(cc->host + first, pitch, cc->dev + first, pitch, (size_t)(y1 - y0) * cc->w * sizeof(float),
-                              (size_t)cc->d, cudaMemcpyDeviceToHost, cc->copy);
-    if (r != cudaSuccess) cc->err = r;
+        r = cudaMemcpy2DAsync(hc->host + first, pitch, hc->dev + first, pitch, (size_t)(y1 - y0) * hc->w * sizeof(float),
+                              (size_t)hc->d, cudaMemcpyDeviceToHost, cs);
+    if (r != cudaSuccess) hc->err = r;
 }
 
 dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float* out, int form)
@@ -1038,43 +1058,57 @@ dol_status dol_edt_mask_3d_host(int w, int h, int d, const uint32_t* mask, float
     if (form != DOL_EDT_SQUARED && form != DOL_EDT_DIST && form != DOL_EDT_SIGNED)
         return fail(DOL_ERR_INVALID_ARG, "form must be DOL_EDT_SQUARED, DOL_EDT_DIST or DOL_EDT_SIGNED");
     if (w > 16384 || h > 16384 || d > 16384) return fail(DOL_ERR_UNSUPPORTED, "EDT dimensions are limited to 16384");
-    OwnStream os, cs;
-    if (cudaStreamCreateWithFlags(&os.st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&cs.st, cudaStreamNonBlocking) != cudaSuccess)
-        return fail(DOL_ERR_CUDA, "cudaStreamCreate failed");
+    OwnStream os, is, o0, o1;
+    for (OwnStream* p : {&os, &is, &o0, &o1})
+        if (cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(DOL_ERR_CUDA, "cudaStreamCreate failed");
     const size_t cells = (size_t)w * h * d;
     const size_t mb = dol_mask_words(w, h, d) * sizeof(uint32_t);
     DevBuf dm, df, dw;
     DOL_TRY(dm.alloc(mb, os.st));
     DOL_TRY(df.alloc(cells * sizeof(float), os.st));
     DOL_TRY(dw.alloc(edt_workspace_bytes(3, w, h, d), os.st));
-    DOL_TRY(copy(dm.p, mask, mb, cudaMemcpyHostToDevice, os.st));
-    ChunkCopy cc{out, static_cast<const float*>(df.p), w, h, d, os.st, cs.st, {}, 0, cudaSuccess};
-    const int chunks = h >= 64 ? 8 : 1;
-    for (int i = 0; i < chunks; i++)
-        if (cudaEventCreateWithFlags(&cc.ev[i], cudaEventDisableTiming) != cudaSuccess) {
-            for (int j = 0; j < i; j++) cudaEventDestroy(cc.ev[j]);
+    // the copy-in stream starts after the allocations it writes into
+    cudaEvent_t start;
+    if (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess)
+        return fail(DOL_ERR_CUDA, "cudaEventCreate failed");
+    cudaEventRecord(start, os.st);
+    cudaStreamWaitEvent(is.st, start, 0);
+    cudaEventDestroy(start);
+    HostCopies hc{mask, static_cast<uint32_t*>(dm.p), out, static_cast<const float*>(df.p), w, h, d,
+                  os.st, is.st, {o0.st, o1.st}, {}, 0, cudaSuccess};
+    const int nev = kHostSlabs + kHostChunks;
+    for (int i = 0; i < nev; i++)
+        if (cudaEventCreateWithFlags(&hc.ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            for (int j = 0; j < i; j++) cudaEventDestroy(hc.ev[j]);
             return fail(DOL_ERR_CUDA, "cudaEventCreate failed");
         }
+    const int slabs = d >= 2 * kHostSlabs ? kHostSlabs : 1;
+    const int chunks = h >= 8 * kHostChunks ? kHostChunks : (h >= 64 ? 8 : 1);
     launch_edt_mask_3d_chunked(static_cast<uint32_t*>(dm.p), static_cast<float*>(df.p), w, h, d, form, dw.p,
-                               ds->err_dev, os.st, chunks, chunk_done, &cc);
+                               ds->err_dev, os.st, slabs, slab_ready, chunks, chunk_done, &hc);
     const cudaError_t le = cudaGetLastError();
-    // the copies must finish before the device buffers are released (the
+    // the copies back must finish before the device buffers are released (the
     // DevBuf destructors free on the compute stream)
-    cudaEvent_t fin;
-    if (cudaEventCreateWithFlags(&fin, cudaEventDisableTiming) == cudaSuccess) {
-        cudaEventRecord(fin, cs.st);
-        cudaStreamWaitEvent(os.st, fin, 0);
-        cudaEventDestroy(fin);
-    } else {
-        cudaStreamSynchronize(cs.st);
+    for (cudaStream_t cs : {o0.st, o1.st}) {
+        cudaEvent_t fin;
+        if (cudaEventCreateWithFlags(&fin, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(fin, cs);
+            cudaStreamWaitEvent(os.st, fin, 0);
+            cudaEventDestroy(fin);
+        } else {
+            cudaStreamSynchronize(cs);
+        }
     }
-    for (int i = 0; i < chunks; i++) cudaEventDestroy(cc.ev[i]);
+    for (int i = 0; i < nev; i++) cudaEventDestroy(hc.ev[i]);
     if (le != cudaSuccess) return fail(DOL_ERR_CUDA, "launch failed: %s", cudaGetErrorString(le));
-    if (cc.err != cudaSuccess) return fail(DOL_ERR_CUDA, "copy to host failed: %s", cudaGetErrorString(cc.err));
-    const dol_status s1 = dol_sync(cs.st);
-    const dol_status s0 = dol_sync(os.st);
-    return s0 != DOL_OK ? s0 : s1;
+    if (hc.err != cudaSuccess) return fail(DOL_ERR_CUDA, "host copy failed: %s", cudaGetErrorString(hc.err));
+    dol_status st = DOL_OK;
+    for (cudaStream_t cs : {is.st, o0.st, o1.st, os.st}) {
+        const dol_status si = dol_sync(cs);
+        if (st == DOL_OK) st = si;
+    }
+    return st;
 }
 
 }  // extern "C"

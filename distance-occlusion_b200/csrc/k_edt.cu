@@ -496,23 +496,33 @@ void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, in
     }
 }
 
-// The 3D mask EDT with the last (z) pass cut into `chunks` launches over ranges
-// of y; after each launch `done(ctx, y0, y1)` runs on the host so the caller can
-// queue work on rows y0..y1-1 of every slice (a copy back to the host that
-// overlaps the remaining launches).
+// The 3D mask EDT in pieces, for a caller that overlaps copies with it: the x
+// and y passes run over `slabs` ranges of z, each after `ready(ctx, z0, z1)`
+// (the caller makes the stream wait for those slices of the mask), and the
+// last (z) pass over `chunks` ranges of y, each followed by `done(ctx, y0, y1)`
+// (the caller queues work on rows y0..y1-1 of every slice, e.g. their copy
+// back to the host).  Both hooks run on the host after / before the launches.
 void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
-                                cudaStream_t st, int chunks, void (*done)(void*, int, int), void* ctx)
+                                cudaStream_t st, int slabs, void (*ready)(void*, int, int), int chunks,
+                                void (*done)(void*, int, int), void* ctx)
 {
-    const long long rows = (long long)h * d;
-    const size_t cells = (size_t)w * rows;
+    const size_t cells = (size_t)w * h * d;
+    const int words = words_per_row(w);
     uint16_t* vx = static_cast<uint16_t*>(ws);
-    const long long blocks = (rows * 32 + 255) / 256, cap = (long long)g_num_sms * 16;
-    k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask, vx, w, rows);
     const size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
     uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
-    line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st);
-    if (chunks < 1) chunks = 1;
-    if (chunks > h) chunks = h;
+    slabs = slabs < 1 ? 1 : (slabs > d ? d : slabs);
+    for (int s = 0; s < slabs; s++) {
+        const int z0 = (int)((long long)d * s / slabs), z1 = (int)((long long)d * (s + 1) / slabs);
+        if (z1 <= z0) continue;
+        if (ready) ready(ctx, z0, z1);
+        const long long rows = (long long)(z1 - z0) * h;
+        const long long blocks = (rows * 32 + 255) / 256, cap = (long long)g_num_sms * 16;
+        k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask + (size_t)z0 * h * words,
+                                                                    vx + (size_t)z0 * h * w, w, rows);
+        line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st, z0, z1 - z0);
+    }
+    chunks = chunks < 1 ? 1 : (chunks > h ? h : chunks);
     for (int c = 0; c < chunks; c++) {
         const int y0 = (int)((long long)h * c / chunks), y1 = (int)((long long)h * (c + 1) / chunks);
         if (y1 <= y0) continue;

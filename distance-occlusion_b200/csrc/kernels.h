@@ -62,7 +62,8 @@ size_t edt_workspace_bytes(int dim, int w, int h, int d);
 void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
                      cudaStream_t st);
 void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, int d, int form, void* ws, int* err,
-                                cudaStream_t st, int chunks, void (*done)(void*, int, int), void* ctx);
+                                cudaStream_t st, int slabs, void (*ready)(void*, int, int), int chunks,
+                                void (*done)(void*, int, int), void* ctx);
 void launch_edt_mask_2d_plain(const uint32_t* mask, float* out, int w, int h, int form, uint16_t* scratch, int sms,
                               cudaStream_t st);
 // faithful float Felzenszwalb (2D, arbitrary input)

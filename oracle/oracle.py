@@ -271,6 +271,52 @@ def sdf_signed_felzenszwalb(mask, dims):
     return (np.sqrt(e_occ) - np.sqrt(e_emp)).astype(np.float32)
 
 
+def edt_exact_thin(mask, dims):
+    """Exact squared EDT in int64 for fields with few rows per line set (h * d
+    small): exact distance along x to the nearest set cell of each row, then the
+    min over all rows of dx^2 + dy^2 + dz^2.  Used where a row is longer than the
+    reference's float envelope keeps exact (about 4096 cells: its q*q passes 2^24
+    and the intersections round), i.e. as the exact EDT rather than the
+    reference's.  Returns int64 with -1 where no set cell exists."""
+    b = mask_to_bool(mask, dims)
+    shp = b.shape
+    w = dims[0]
+    rows = b.reshape(-1, w)
+    inf = np.int64(1) << 60
+    xs = np.arange(w)
+    dx = np.full(rows.shape, inf, np.int64)
+    for r in range(rows.shape[0]):
+        idx = np.nonzero(rows[r])[0]
+        if idx.size:
+            pos = np.searchsorted(idx, xs)
+            left = np.where(pos > 0, xs - idx[np.maximum(pos - 1, 0)], inf)
+            right = np.where(pos < idx.size, idx[np.minimum(pos, idx.size - 1)] - xs, inf)
+            dx[r] = np.minimum(left, right)
+    h = dims[1]
+    d = dims[2] if len(dims) == 3 else 1
+    out = np.full(rows.shape, inf, np.int64)
+    for r in range(rows.shape[0]):
+        z, y = divmod(r, h)
+        for r2 in range(rows.shape[0]):
+            z2, y2 = divmod(r2, h)
+            cand = np.where(dx[r2] < inf, dx[r2] ** 2 + (y - y2) ** 2 + (z - z2) ** 2, inf)
+            out[r] = np.minimum(out[r], cand)
+    out = np.where(out >= inf, -1, out)
+    return out.reshape(shp)
+
+
+def sdf_signed_exact_thin(mask, dims):
+    """Signed field (distance to set cells minus distance to clear cells) from the
+    exact EDT of edt_exact_thin, in float32 as the GPU forms it."""
+    b = mask_to_bool(mask, dims)
+    inv = bool_to_mask(~b) if b.ndim == 2 else bool_to_mask(~b)
+    big = np.float32(np.finfo(np.float32).max)
+    def f(e):
+        return np.where(e < 0, big, e.astype(np.float32)).astype(np.float32)
+    e_occ, e_emp = f(edt_exact_thin(mask, dims)), f(edt_exact_thin(inv, dims))
+    return (np.sqrt(e_occ) - np.sqrt(e_emp)).astype(np.float32)
+
+
 def edt_brute(mask, dims):
     d3 = list(dims) + [1] * (3 - len(dims))
     out = np.empty(d3[0] * d3[1] * d3[2], dtype=np.float32)

@@ -71,6 +71,22 @@ def test_delta_methods(dol, O, cuda, dims, method):
             np.testing.assert_array_equal(host(got), want, err_msg=f"{method} cw{cw} p{p} dims{dims}")
 
 
+@pytest.mark.parametrize("method", ["danielsson", "fastsweep", "jumpflood"])
+@pytest.mark.parametrize("dims", [(4096, 6), (2049, 9), (2048, 3, 3), (1025, 2, 4)])
+def test_delta_methods_widest_rows(dol, O, cuda, dims, method):
+    """Rows at and around the sweep engines' limits (4096 cells in 2D; 2048 for
+    3D FastSweep), past the block schedule's 2048, odd lengths."""
+    rng = np.random.default_rng(sum(dims) + len(method) + 1)
+    for p in (0.001, 0.3):
+        m = rand_mask(O, rng, dims, p)
+        for cw in (1, 2):
+            start = O.init_deltas(m, dims) if cw == 1 else O.border_init(m, dims)
+            want = O.propagate(method, start, dims, cw)
+            got = dol.propagate(method, dev(cuda, start), dims, cw)
+            dol.sync()
+            np.testing.assert_array_equal(host(got), want, err_msg=f"{method} cw{cw} p{p} dims{dims}")
+
+
 @pytest.mark.parametrize("dims", [(1024, 1024)])
 def test_config1_against_reference_digests(dol, O, cuda, dims):
     with open(os.path.join(HERE, "golden", "golden_digests.json")) as f:
@@ -206,7 +222,7 @@ def test_edt_mask_host_chunked(dol, O, cuda, dims):
 
 
 @pytest.mark.parametrize("dims", [(8, 1000, 3), (16, 300, 37), (24, 5, 777), (8, 2049, 2), (40, 3, 1029),
-                                  (2000, 8), (64, 1027)])
+                                  (2000, 8), (64, 1027), (4096, 5), (8, 4096, 2)])
 def test_edt_mask_long_lines(dol, O, cuda, dims):
     """Long y / z lines: several TMA boxes, lengths off the 4 / 32 grid, runs
     longer than a word, searches that reach the line ends."""
@@ -219,6 +235,23 @@ def test_edt_mask_long_lines(dol, O, cuda, dims):
         want_sq = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims)
         same_float(host(dol.edt_mask(md, dims, dol.EDT_SQUARED)), want_sq)
         same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
+
+
+@pytest.mark.parametrize("dims", [(16384, 4), (16384, 3, 2), (12345, 5), (5000, 3)])
+def test_edt_mask_rows_beyond_float_exactness(dol, O, cuda, dims):
+    """Rows longer than 4096 cells: the reference's float envelope is no longer
+    exact there (its q*q passes 2^24; an all-set 5000 x 3 image already gets
+    nonzero distances), so the check is the exact EDT, which the library keeps
+    computing in integers (16384-cell rows also take the x pass's chunk carries)."""
+    rng = np.random.default_rng(sum(dims) + 11)
+    big = np.float32(np.finfo(np.float32).max)
+    for p in (0.0, 0.0005, 0.01, 0.3, 1.0):
+        m = rand_mask(O, rng, dims, p)
+        md = dev(cuda, m)
+        ex = O.edt_exact_thin(m, dims)
+        want_sq = np.where(ex < 0, big, ex.astype(np.float32)).astype(np.float32)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SQUARED)), want_sq)
+        same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_exact_thin(m, dims))
 
 
 @pytest.mark.parametrize("dims", [(1, 1), (7, 1), (1, 7), (33, 17), (64, 48), (200, 130)])

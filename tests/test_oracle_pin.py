@@ -182,6 +182,30 @@ def test_chamfer_oracle_vs_reference(O, dims):
         np.testing.assert_array_equal(O.chamfer(f, dims)[0], O.chamfer(f, dims, use_ref=True)[0])
 
 
+def test_reference_felzenszwalb_exact_range(O):
+    """Where the reference's float Felzenszwalb stops being the exact EDT: rows of
+    up to 4096 cells give the exact squared EDT (every intermediate an integer
+    below 2^24), longer rows do not (an all-set 5000 x 3 image comes back with
+    nonzero distances).  The integer EDT used to check the GPU beyond 4096 agrees
+    with the reference inside that range."""
+    if O.ref() is None:
+        pytest.skip("reference build (oracle/_ref) not available")
+    big = np.float32(np.finfo(np.float32).max)
+    zero = O.felzenszwalb(np.zeros((3, 4096), np.float32), (4096, 3), use_ref=True)
+    assert not zero.any()
+    off = O.felzenszwalb(np.zeros((3, 5000), np.float32), (5000, 3), use_ref=True)
+    assert off.any()
+    rng = np.random.default_rng(4)
+    for dims in ((300, 4), (100, 3, 2), (4096, 3)):
+        for p in (0.0, 0.01, 0.4, 1.0):
+            m = _rand_mask(rng, dims, p, False)
+            b = O.mask_to_bool(m, dims)
+            want = O.felzenszwalb(np.where(b, np.float32(0), big).astype(np.float32), dims, use_ref=True)
+            ex = O.edt_exact_thin(m, dims)
+            got = np.where(ex < 0, big, ex.astype(np.float32)).astype(np.float32)
+            np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 def test_felzenszwalb_is_exact_edt(O):
     """The float envelope returns the exact squared EDT (so any exact EDT matches it)."""
     rng = np.random.default_rng(5)

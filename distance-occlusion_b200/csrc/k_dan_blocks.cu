@@ -439,12 +439,15 @@ static bool run_phase(DanBlk& p, void* dl, cudaStream_t st)
         return false;
     const int resident = per_sm * g_num_sms;
     // slices per block: long enough that few rounds are needed, short enough
-    // that about four block columns per resident CTA keep every SM busy
+    // that about four block columns per resident CTA keep every SM busy, and
+    // at most 16 (on 1024^3 noise, 16 slices ran 686 -> 553 ms against the
+    // 110 the column rule gives; 32 and 64 were slower than 16)
     int Z = tune_get(kTuneDanSlices, p.w);
     if (Z < 1) {
         const long long cols = 4LL * resident;
         Z = (int)((long long)p.nchain * p.nc / cols);
         if (Z < 1) Z = 1;
+        if (Z > 16) Z = 16;
     }
     if (Z > p.nchain) Z = p.nchain;
     p.Z = Z;

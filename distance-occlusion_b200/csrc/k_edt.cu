@@ -274,8 +274,18 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
 // state-specific arrays: F_s[p] is the cell's value (v or e) when its state is
 // s and 0 otherwise, so for a cell of state s every probe is one load, one
 // multiply-add (or add) and one min -- a cell of the other state at distance k
-// contributes exactly k^2.  The symmetric part of the walk runs without bounds
-// checks; a warp covers 8 columns x 4 adjacent positions.
+// contributes exactly k^2.  Each array carries kPadRows rows of "no cell"
+// sentinels before and after the line (positions n .. rows-1 too), so the walk
+// outwards from a cell runs on both sides with one test per two distances
+// until it either ends or passes kPadRows beyond the nearer line end; only
+// then does it continue on the far side alone.  A warp covers 8 columns x 4
+// adjacent positions.
+//
+// Layouts (kMode): 0 reads and writes [z][y][x]; 1 (y pass of a volume) writes
+// its uint32 output as [y][x/8][z][8], so that 2 (the z pass) reads every
+// 8-column z line as one contiguous 32-byte-row tile.
+constexpr int kPadRows = 32;
+
 template <typename TIn>
 __device__ __forceinline__ uint32_t sq_val(TIn v)
 {
@@ -288,7 +298,13 @@ __device__ __forceinline__ uint32_t add_sq(TIn v, uint32_t k2)
     return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v + k2 : (uint32_t)v + k2;
 }
 
-template <typename TIn, bool kFinal, int TX>
+template <typename TIn, int TX>
+static size_t tma_tile_bytes(int n)
+{
+    return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn);
+}
+
+template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
                                                       int along_z, int form, int* err, int outer0)
@@ -296,17 +312,28 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
     const int rows = nbox * 256;
-    TIn* F0 = reinterpret_cast<TIn*>(smem_raw);   // [rows][TX], first the raw tile
-    TIn* F1 = F0 + rows * TX;                      // [rows][TX]
+    TIn* F0 = reinterpret_cast<TIn*>(smem_raw) + kPadRows * TX;   // rows -kPadRows .. rows+kPadRows-1, first the raw tile
+    TIn* F1 = F0 + (rows + 2 * kPadRows) * TX;                      // the same for state 1
     __shared__ __align__(8) uint64_t bar;
-    const int x0 = blockIdx.x * TX;
-    const int outer = blockIdx.y + outer0;
+    int x0, outer, line = 0;
+    if (kMode == 2) {
+        // one block per (y, 8-column group) of the [y][x/8][z][8] array
+        const int wb = w >> 3;
+        line = blockIdx.x + outer0 * wb;
+        outer = line / wb;
+        x0 = (line - outer * wb) * 8;
+    } else {
+        x0 = blockIdx.x * TX;
+        outer = blockIdx.y + outer0;
+    }
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_expect_tx(&bar, (uint32_t)(rows * TX * sizeof(TIn)));
         for (int b = 0; b < nbox; b++) {
-            if (along_z)
+            if (kMode == 2)
+                tma_load_3d(F0 + b * 256 * TX, &map, 0, b * 256, line, &bar);
+            else if (along_z)
                 tma_load_3d(F0 + b * 256 * TX, &map, x0, outer, b * 256, &bar);
             else
                 tma_load_3d(F0 + b * 256 * TX, &map, x0, b * 256, outer, &bar);
@@ -318,15 +345,26 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         if (threadIdx.x == 0) atomicExch(err, 2);
         return;
     }
-    // split by state: the top bit is the state, the rest the value
+    // split by state (the top bit is the state, the rest the value); positions
+    // n .. rows + kPadRows - 1 and the kPadRows rows before 0 become sentinels
     constexpr int kTop = sizeof(TIn) * 8 - 1;
     constexpr uint32_t kVal = (1u << kTop) - 1u;
-    for (int i = threadIdx.x; i < n * TX; i += blockDim.x) {
-        uint32_t x = (uint32_t)F0[i];
-        uint32_t v = x & kVal;
-        bool st = (x >> kTop) & 1u;
-        F0[i] = (TIn)(st ? 0u : v);
-        F1[i] = (TIn)(st ? v : 0u);
+    const TIn kSent = (TIn)kVal;
+    for (int i = threadIdx.x; i < (rows + kPadRows) * TX; i += blockDim.x) {
+        if (i < n * TX) {
+            const uint32_t x = (uint32_t)F0[i];
+            const uint32_t v = x & kVal;
+            const bool st = (x >> kTop) & 1u;
+            F0[i] = (TIn)(st ? 0u : v);
+            F1[i] = (TIn)(st ? v : 0u);
+        } else {
+            F0[i] = kSent;
+            F1[i] = kSent;
+        }
+        if (i < kPadRows * TX) {
+            F0[i - kPadRows * TX] = kSent;
+            F1[i - kPadRows * TX] = kSent;
+        }
     }
     __syncthreads();
 
@@ -339,47 +377,51 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     const int qstep = 4 * (nw / kGroups);
     const int x = x0 + col;
     if (x >= w) return;
-    const long long base = (long long)outer * outer_stride + x;
+    const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
+                                      : (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
     for (int q = 4 * (wi / kGroups) + sub; q < n; q += qstep) {
         const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
         const TIn* A = (s ? F1 : F0) + col;
         uint32_t best = sq_val<TIn>(A[q * TX]);
-        const int lmax = q, rmax = n - 1 - q, kmin = min(lmax, rmax);
-        int k = 1;
-        uint32_t k2 = 1;   // k^2
+        const int kmin = min(q, n - 1 - q);
+        // both sides, two distances per trip, while k^2 < best and k stays
+        // within kPadRows of the nearer line end (sentinels past it)
+        const uint32_t kcap = (uint32_t)(kmin + kPadRows);
+        const uint32_t cap2 = kcap * kcap;
+        uint32_t k2 = 1, t = 3;   // k^2 and 2k + 1 for the next distance k
+        uint32_t lim = min(best, cap2);
         const TIn* pl = A + (q - 1) * TX;
         const TIn* pr = A + (q + 1) * TX;
-        // both sides, two distances per trip (at most one probe past the stop,
-        // which cannot lower the minimum below its exact value)
-        for (; k + 1 <= kmin && k2 < best; k += 2) {
-            const uint32_t k2b = k2 + 2 * k + 1;   // (k+1)^2
+        while (k2 < lim) {
+            const uint32_t k2b = k2 + t;   // (k+1)^2
             best = min(best, min(add_sq<TIn>(pl[0], k2), add_sq<TIn>(pr[0], k2)));
             best = min(best, min(add_sq<TIn>(pl[-TX], k2b), add_sq<TIn>(pr[TX], k2b)));
             pl -= 2 * TX;
             pr += 2 * TX;
-            k2 = k2b + 2 * k + 3;   // (k+2)^2
+            k2 = k2b + t + 2;   // (k+2)^2
+            t += 4;
+            lim = min(best, cap2);
         }
-        if (k <= kmin && k2 < best) {
-            best = min(best, min(add_sq<TIn>(pl[0], k2), add_sq<TIn>(pr[0], k2)));
-            pl -= TX;
-            pr += TX;
-            k2 += 2 * k + 1;
-            k++;
+        if (k2 < best) {
+            // stopped more than kPadRows past the nearer end: the far side alone
+            int k = (int)(t >> 1);
+            if (q <= n - 1 - q) {
+                for (; k <= n - 1 - q && k2 < best; k++) {
+                    best = min(best, add_sq<TIn>(*pr, k2));
+                    pr += TX;
+                    k2 += 2 * k + 1;
+                }
+            } else {
+                for (; k <= q && k2 < best; k++) {
+                    best = min(best, add_sq<TIn>(*pl, k2));
+                    pl -= TX;
+                    k2 += 2 * k + 1;
+                }
+            }
         }
-        // one side left
-        for (; k <= lmax && k2 < best; k++) {
-            best = min(best, add_sq<TIn>(*pl, k2));
-            pl -= TX;
-            k2 += 2 * k + 1;
-        }
-        for (; k <= rmax && k2 < best; k++) {
-            best = min(best, add_sq<TIn>(*pr, k2));
-            pr += TX;
-            k2 += 2 * k + 1;
-        }
-        put_line_value<kFinal>(out, base + q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
+        put_line_value<kFinal>(out, base + (long long)q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }
 }
 
@@ -399,13 +441,45 @@ static void line_pass_plain(const TIn* in, void* out, int w, int n, long long st
     }
 }
 
+// Tensor map of the TMA line kernels: lines along y (along_z = 0) or z of a
+// w x h x d array, TX columns per box row; mode 2: the [y][x/8][z][8] array.
+template <typename TIn, int TX>
+static bool line_map(CUtensorMap* map, const TIn* in, int w, int h, int d, int along_z, int mode)
+{
+    const CUtensorMapDataType type = sizeof(TIn) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+    if (mode == 2) {
+        const uint64_t dims[3] = {8, (uint64_t)d, (uint64_t)(w / 8) * h};
+        const uint64_t strides[2] = {8 * sizeof(TIn), (uint64_t)d * 8 * sizeof(TIn)};
+        const uint32_t box[3] = {8, 256, 1};
+        return encode_map_3d(map, in, type, dims, strides, box);
+    }
+    const uint64_t plane = (uint64_t)w * h;
+    const uint64_t dims[3] = {(uint64_t)w, (uint64_t)h, (uint64_t)d};
+    const uint64_t strides[2] = {(uint64_t)w * sizeof(TIn), plane * sizeof(TIn)};
+    const uint32_t box[3] = {(uint32_t)TX, along_z ? 1u : 256u, along_z ? 256u : 1u};
+    return encode_map_3d(map, in, type, dims, strides, box);
+}
+
+// True when a volume's y pass can write, and its z pass read, the
+// [y][x/8][z][8] array: 8 | w, both line tiles fit, both maps encode.
+static bool blocked_layout_ok(const uint16_t* vx, const uint32_t* ey, int w, int h, int d)
+{
+    if (w % 8 != 0 || d > 65535) return false;
+    if (tma_tile_bytes<uint16_t, 16>(h) > 200 * 1024 || tma_tile_bytes<uint32_t, 8>(d) > 200 * 1024) return false;
+    if ((long long)(w / 8) * h > 0x7FFFFFFFLL) return false;
+    if (((uintptr_t)vx % 16) != 0 || ((uintptr_t)ey % 16) != 0) return false;
+    CUtensorMap m;
+    return line_map<uint16_t, 16>(&m, vx, w, h, d, 0, 1) && line_map<uint32_t, 8>(&m, ey, w, h, d, 1, 2);
+}
+
 // Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
 // of a w x h x d array; outer indices outer0 .. outer0 + nouter - 1 (nouter < 0:
 // all).  TMA needs 16-byte row pitches and a tile that fits in shared memory;
-// otherwise the plain form runs.
+// otherwise the plain form runs.  mode 1 / 2 (blocked y-pass output / z-pass
+// input) only after blocked_layout_ok.
 template <typename TIn, bool kFinal>
 static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z, int form, int* err, cudaStream_t st,
-                      int outer0 = 0, int nouter = -1)
+                      int outer0 = 0, int nouter = -1, int mode = 0)
 {
     const int n = along_z ? d : h;
     const long long plane = (long long)w * h;
@@ -413,21 +487,32 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const long long outer = nouter >= 0 ? nouter : (along_z ? h : d);
     const long long outer_stride = along_z ? w : plane;
     constexpr int TX = sizeof(TIn) == 2 ? 16 : 8;   // 32-byte box rows either way
-    const int nbox = (n + 255) / 256;
-    const size_t tile_bytes = 2 * (size_t)nbox * 256 * TX * sizeof(TIn);
+    const size_t tile_bytes = tma_tile_bytes<TIn, TX>(n);
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
+    const int tv = tune_get(kTuneEdt, w);
+    const int threads = tv == 256 ? 256 : 512;
     CUtensorMap map;
+    if (mode == 1) {
+        if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) return;   // blocked_layout_ok encoded it already
+        auto kern = k_edt_line_tma<TIn, kFinal, TX, 1>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+        dim3 grid((w + TX - 1) / TX, (unsigned)outer);
+        kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0);
+        return;
+    }
+    if (mode == 2) {
+        if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 2)) return;
+        auto kern = k_edt_line_tma<TIn, kFinal, 8, 2>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+        const unsigned blocks = (unsigned)(outer * (w / 8));
+        kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0);
+        return;
+    }
     if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {
-        const uint64_t dims[3] = {(uint64_t)w, (uint64_t)h, (uint64_t)d};
-        const uint64_t strides[2] = {(uint64_t)w * sizeof(TIn), (uint64_t)plane * sizeof(TIn)};
-        const uint32_t box[3] = {(uint32_t)TX, along_z ? 1u : 256u, along_z ? 256u : 1u};
-        const CUtensorMapDataType type = sizeof(TIn) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
-        if (encode_map_3d(&map, in, type, dims, strides, box)) {
-            auto kern = k_edt_line_tma<TIn, kFinal, TX>;
+        if (line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) {
+            auto kern = k_edt_line_tma<TIn, kFinal, TX, 0>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
-            const int tv = tune_get(kTuneEdt, w);
-            const int threads = tv == 256 ? 256 : 512;
             kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0);
             return;
         }
@@ -487,12 +572,13 @@ void launch_edt_mask(int dim, const uint32_t* mask, float* out, int w, int h, in
     } else {
         size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
         uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
+        const bool blk = blocked_layout_ok(vx, ey, w, h, d);
         {
             ProfScope ps("edt_y", st);
-            line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st);   // y lines
+            line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st, 0, -1, blk ? 1 : 0);   // y lines
         }
         ProfScope ps("edt_z_final", st);
-        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st);   // z lines
+        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st, 0, -1, blk ? 2 : 0);   // z lines
     }
 }
 
@@ -511,6 +597,7 @@ void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, 
     uint16_t* vx = static_cast<uint16_t*>(ws);
     const size_t off = (cells * sizeof(uint16_t) + 255) & ~(size_t)255;
     uint32_t* ey = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + off);
+    const bool blk = blocked_layout_ok(vx, ey, w, h, d);
     slabs = slabs < 1 ? 1 : (slabs > d ? d : slabs);
     for (int s = 0; s < slabs; s++) {
         const int z0 = (int)((long long)d * s / slabs), z1 = (int)((long long)d * (s + 1) / slabs);
@@ -520,13 +607,13 @@ void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, 
         const long long blocks = (rows * 32 + 255) / 256, cap = (long long)g_num_sms * 16;
         k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask + (size_t)z0 * h * words,
                                                                     vx + (size_t)z0 * h * w, w, rows);
-        line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st, z0, z1 - z0);
+        line_pass<uint16_t, false>(vx, ey, w, h, d, 0, form, err, st, z0, z1 - z0, blk ? 1 : 0);
     }
     chunks = chunks < 1 ? 1 : (chunks > h ? h : chunks);
     for (int c = 0; c < chunks; c++) {
         const int y0 = (int)((long long)h * c / chunks), y1 = (int)((long long)h * (c + 1) / chunks);
         if (y1 <= y0) continue;
-        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st, y0, y1 - y0);
+        line_pass<uint32_t, true>(ey, out, w, h, d, 1, form, err, st, y0, y1 - y0, blk ? 2 : 0);
         if (done) done(ctx, y0, y1);
     }
 }

@@ -13,9 +13,11 @@
 //   y pass  per column: e(y) = min over y' of (y-y')^2 + f(y'), where f(y') is 0
 //           for cells of the opposite state and v(y')^2 otherwise.  The search
 //           walks outwards from y and stops once k^2 >= the best so far, which
-//           is exact because f >= 0.  Columns are staged in shared memory, 32
-//           adjacent x per CTA so global accesses are whole 64/128-byte rows.
-//   z pass  the same along z on the y-pass output (uint32, state in bit 31).
+//           is exact because f >= 0.  Whole columns of 16 adjacent x are
+//           staged in shared memory by TMA.
+//   z pass  the same along z on the y-pass output (uint32, state in bit 31),
+//           which a volume of width 8k stores as [y][x/8][z][8] so that each
+//           8-column z line is one contiguous tile.
 //
 // Keeping "distance to the opposite state" per cell serves both forms at once:
 // for an empty cell it is the distance to the nearest set cell (the unsigned

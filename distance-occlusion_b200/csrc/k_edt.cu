@@ -300,6 +300,29 @@ __device__ __forceinline__ uint32_t add_sq(TIn v, uint32_t k2)
     return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v + k2 : (uint32_t)v + k2;
 }
 
+// The rest of a walk on the far side of cell q once the near side is done:
+// distances k.. with k2 = k^2, pl / pr at q - k / q + k; ends at the line end
+// or when k^2 reaches the best value.
+template <typename TIn, int TX>
+__device__ __forceinline__ uint32_t far_side(uint32_t best, int q, int n, int k, uint32_t k2, const TIn* pl,
+                                             const TIn* pr)
+{
+    if (q <= n - 1 - q) {
+        for (; k <= n - 1 - q && k2 < best; k++) {
+            best = min(best, add_sq<TIn>(*pr, k2));
+            pr += TX;
+            k2 += 2 * k + 1;
+        }
+    } else {
+        for (; k <= q && k2 < best; k++) {
+            best = min(best, add_sq<TIn>(*pl, k2));
+            pl -= TX;
+            k2 += 2 * k + 1;
+        }
+    }
+    return best;
+}
+
 template <typename TIn, int TX>
 static size_t tma_tile_bytes(int n)
 {
@@ -370,60 +393,64 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     }
     __syncthreads();
 
-    // a warp covers 8 columns x 4 positions (a compact footprint: neighbouring
-    // cells have similar search lengths, and the 32 probes of a step fall in
-    // distinct shared-memory banks); TX / 8 column groups per CTA
+    // a warp covers 8 columns x 8 positions, each lane two cells of its
+    // column 4 apart, both walked in one loop (a compact footprint:
+    // neighbouring cells have similar search lengths; the probes of each half
+    // of a step, 8 columns x 4 adjacent positions, fall in distinct
+    // shared-memory banks); TX / 8 column groups per CTA
     constexpr int kGroups = TX / 8;
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
     const int col = (wi % kGroups) * 8 + (lane & 7), sub = lane >> 3;
-    const int qstep = 4 * (nw / kGroups);
+    const int qstep = 8 * (nw / kGroups);
     const int x = x0 + col;
     if (x >= w) return;
     const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
                                       : (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-    for (int q = 4 * (wi / kGroups) + sub; q < n; q += qstep) {
-        const uint32_t s = F1[q * TX + col] != 0;   // every own value is >= 1
-        const TIn* A = (s ? F1 : F0) + col;
-        uint32_t best = sq_val<TIn>(A[q * TX]);
-        const int kmin = min(q, n - 1 - q);
-        // both sides, two distances per trip, while k^2 < best and k stays
-        // within kPadRows of the nearer line end (sentinels past it)
-        const uint32_t kcap = (uint32_t)(kmin + kPadRows);
-        const uint32_t cap2 = kcap * kcap;
+    for (int qa = 8 * (wi / kGroups) + sub; qa < n; qa += qstep) {
+        const bool has_b = qa + 4 < n;
+        const int qb = has_b ? qa + 4 : qa;   // without a second cell the lane walks the first twice
+        const uint32_t sa = F1[qa * TX + col] != 0, sb = F1[qb * TX + col] != 0;   // every own value is >= 1
+        const TIn* Aa = (sa ? F1 : F0) + col;
+        const TIn* Ab = (sb ? F1 : F0) + col;
+        uint32_t besta = sq_val<TIn>(Aa[qa * TX]), bestb = sq_val<TIn>(Ab[qb * TX]);
+        // both sides, two distances per trip, while k^2 < best for either cell
+        // and k stays within kPadRows - 4 of that cell's nearer line end (the
+        // other cell is at most 4 positions away, so neither walks past the
+        // sentinels)
+        const uint32_t kca = (uint32_t)(min(qa, n - 1 - qa) + kPadRows - 4);
+        const uint32_t kcb = (uint32_t)(min(qb, n - 1 - qb) + kPadRows - 4);
+        const uint32_t cap2a = kca * kca, cap2b = kcb * kcb;
         uint32_t k2 = 1, t = 3;   // k^2 and 2k + 1 for the next distance k
-        uint32_t lim = min(best, cap2);
-        const TIn* pl = A + (q - 1) * TX;
-        const TIn* pr = A + (q + 1) * TX;
+        uint32_t lim = max(min(besta, cap2a), min(bestb, cap2b));
+        const TIn* pla = Aa + (qa - 1) * TX;
+        const TIn* pra = Aa + (qa + 1) * TX;
+        const TIn* plb = Ab + (qb - 1) * TX;
+        const TIn* prb = Ab + (qb + 1) * TX;
         while (k2 < lim) {
             const uint32_t k2b = k2 + t;   // (k+1)^2
-            best = min(best, min(add_sq<TIn>(pl[0], k2), add_sq<TIn>(pr[0], k2)));
-            best = min(best, min(add_sq<TIn>(pl[-TX], k2b), add_sq<TIn>(pr[TX], k2b)));
-            pl -= 2 * TX;
-            pr += 2 * TX;
+            besta = min(besta, min(add_sq<TIn>(pla[0], k2), add_sq<TIn>(pra[0], k2)));
+            bestb = min(bestb, min(add_sq<TIn>(plb[0], k2), add_sq<TIn>(prb[0], k2)));
+            besta = min(besta, min(add_sq<TIn>(pla[-TX], k2b), add_sq<TIn>(pra[TX], k2b)));
+            bestb = min(bestb, min(add_sq<TIn>(plb[-TX], k2b), add_sq<TIn>(prb[TX], k2b)));
+            pla -= 2 * TX;
+            pra += 2 * TX;
+            plb -= 2 * TX;
+            prb += 2 * TX;
             k2 = k2b + t + 2;   // (k+2)^2
             t += 4;
-            lim = min(best, cap2);
+            lim = max(min(besta, cap2a), min(bestb, cap2b));
         }
-        if (k2 < best) {
-            // stopped more than kPadRows past the nearer end: the far side alone
-            int k = (int)(t >> 1);
-            if (q <= n - 1 - q) {
-                for (; k <= n - 1 - q && k2 < best; k++) {
-                    best = min(best, add_sq<TIn>(*pr, k2));
-                    pr += TX;
-                    k2 += 2 * k + 1;
-                }
-            } else {
-                for (; k <= q && k2 < best; k++) {
-                    best = min(best, add_sq<TIn>(*pl, k2));
-                    pl -= TX;
-                    k2 += 2 * k + 1;
-                }
-            }
+        // a cell whose walk stopped at its cap (more than kPadRows - 4 past its
+        // nearer end) goes on along the far side alone
+        const int k = (int)(t >> 1);
+        if (k2 < besta) besta = far_side<TIn, TX>(besta, qa, n, k, k2, pla, pra);
+        put_line_value<kFinal>(out, base + (long long)qa * stride, sa, besta >= kNone ? 0xFFFFFFFFu : besta, form);
+        if (has_b) {
+            if (k2 < bestb) bestb = far_side<TIn, TX>(bestb, qb, n, k, k2, plb, prb);
+            put_line_value<kFinal>(out, base + (long long)qb * stride, sb, bestb >= kNone ? 0xFFFFFFFFu : bestb, form);
         }
-        put_line_value<kFinal>(out, base + (long long)q * stride, s, best >= kNone ? 0xFFFFFFFFu : best, form);
     }
 }
 

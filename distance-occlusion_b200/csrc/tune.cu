@@ -166,6 +166,12 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     }
     if (kind == kTuneDan3) td = d < 32 ? d : 32;   // whole slices: the block schedule's row blocks
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);
+    if (kind == kTuneEdt) {
+        // the EDT's line kernels are what the value picks, and their cost per
+        // CTA depends on the y and z line lengths: narrow the volume along x
+        // (independent column tiles) before shortening the lines
+        while ((long long)tw * th * td > (1LL << 26) && tw > 64) tw = ((tw / 2 + 15) / 16) * 16;
+    }
     if (kind == kTuneJfa3 || kind == kTuneEdt || kind == kTuneDanRows || kind == kTuneDanSlices) {
         while ((long long)tw * th * td > (1LL << 26) && td > 1) td = (td + 1) / 2;
     }
@@ -249,8 +255,13 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     int best_v = 0;
     float best_t = FLT_MAX;
     const int saved = tune_get(kind, w);
+    // a narrowed synthetic volume looks its value up under its own width:
+    // give it each candidate too, and put its entry back afterwards
+    const bool other_key = bucket_of(tw) != bucket_of(w);
+    const int saved_tw = tune_get(kind, tw);
     for (int v : candidates(kind, w)) {
         tune_put(kind, w, v);
+        if (other_key) tune_put(kind, tw, v);
         run_once();   // warm-up
         float t_best = FLT_MAX;
         for (int rep = 0; rep < 2; rep++) {
@@ -268,6 +279,7 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
         }
     }
     tune_put(kind, w, best_v ? best_v : saved);
+    if (other_key) tune_put(kind, tw, saved_tw);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     for (void* p : {dm, dl, tmp, ws, (void*)err})

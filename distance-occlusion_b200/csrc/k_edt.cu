@@ -430,10 +430,22 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         const TIn* prb = Ab + (qb + 1) * TX;
         while (k2 < lim) {
             const uint32_t k2b = k2 + t;   // (k+1)^2
-            besta = min(besta, min(add_sq<TIn>(pla[0], k2), add_sq<TIn>(pra[0], k2)));
-            bestb = min(bestb, min(add_sq<TIn>(plb[0], k2), add_sq<TIn>(prb[0], k2)));
-            besta = min(besta, min(add_sq<TIn>(pla[-TX], k2b), add_sq<TIn>(pra[TX], k2b)));
-            bestb = min(bestb, min(add_sq<TIn>(plb[-TX], k2b), add_sq<TIn>(prb[TX], k2b)));
+            // three-way minimum (u16) and fused add-min (u32): the DPX integer intrinsics
+            if (sizeof(TIn) == 2) {
+                besta = __vimin3_u32(besta, add_sq<TIn>(pla[0], k2), add_sq<TIn>(pra[0], k2));
+                bestb = __vimin3_u32(bestb, add_sq<TIn>(plb[0], k2), add_sq<TIn>(prb[0], k2));
+                besta = __vimin3_u32(besta, add_sq<TIn>(pla[-TX], k2b), add_sq<TIn>(pra[TX], k2b));
+                bestb = __vimin3_u32(bestb, add_sq<TIn>(plb[-TX], k2b), add_sq<TIn>(prb[TX], k2b));
+            } else {
+                besta = __viaddmin_u32((uint32_t)pla[0], k2, besta);
+                bestb = __viaddmin_u32((uint32_t)plb[0], k2, bestb);
+                besta = __viaddmin_u32((uint32_t)pra[0], k2, besta);
+                bestb = __viaddmin_u32((uint32_t)prb[0], k2, bestb);
+                besta = __viaddmin_u32((uint32_t)pla[-TX], k2b, besta);
+                bestb = __viaddmin_u32((uint32_t)plb[-TX], k2b, bestb);
+                besta = __viaddmin_u32((uint32_t)pra[TX], k2b, besta);
+                bestb = __viaddmin_u32((uint32_t)prb[TX], k2b, bestb);
+            }
             pla -= 2 * TX;
             pra += 2 * TX;
             plb -= 2 * TX;

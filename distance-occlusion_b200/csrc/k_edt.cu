@@ -329,6 +329,19 @@ static size_t tma_tile_bytes(int n)
     return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn);
 }
 
+// One 32-bit word of a staged tile split by state: its cells (two uint16 or
+// one uint32, the state in each cell's top bit) go to *f0 when clear, *f1
+// when set, 0 in the other; vmask holds every cell's value bits.
+template <typename TIn>
+__device__ __forceinline__ void split_word(uint32_t x, uint32_t vmask, uint32_t* f0, uint32_t* f1)
+{
+    const uint32_t v = x & vmask;
+    const uint32_t st = x & ~vmask;                                                 // the state bits
+    const uint32_t m = sizeof(TIn) == 2 ? (st >> 15) * 0xFFFFu : 0u - (st >> 31);   // all of a set cell's bits
+    *f0 = v & ~m;
+    *f1 = v & m;
+}
+
 template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
@@ -370,26 +383,31 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         if (threadIdx.x == 0) atomicExch(err, 2);
         return;
     }
-    // split by state (the top bit is the state, the rest the value); positions
-    // n .. rows + kPadRows - 1 and the kPadRows rows before 0 become sentinels
-    constexpr int kTop = sizeof(TIn) * 8 - 1;
-    constexpr uint32_t kVal = (1u << kTop) - 1u;
-    const TIn kSent = (TIn)kVal;
-    for (int i = threadIdx.x; i < (rows + kPadRows) * TX; i += blockDim.x) {
-        if (i < n * TX) {
-            const uint32_t x = (uint32_t)F0[i];
-            const uint32_t v = x & kVal;
-            const bool st = (x >> kTop) & 1u;
-            F0[i] = (TIn)(st ? 0u : v);
-            F1[i] = (TIn)(st ? v : 0u);
-        } else {
-            F0[i] = kSent;
-            F1[i] = kSent;
-        }
-        if (i < kPadRows * TX) {
-            F0[i - kPadRows * TX] = kSent;
-            F1[i - kPadRows * TX] = kSent;
-        }
+    // split by state (the top bit is the state, the rest the value), 16 bytes
+    // at a time; positions n .. rows + kPadRows - 1 and the kPadRows rows
+    // before 0 become sentinels.  A row is TX * sizeof(TIn) = 32 bytes.
+    constexpr int kVecRow = TX * (int)sizeof(TIn) / 16;
+    uint4* V0 = reinterpret_cast<uint4*>(F0);
+    uint4* V1 = reinterpret_cast<uint4*>(F1);
+    const uint32_t sw = sizeof(TIn) == 2 ? 0x7FFF7FFFu : 0x7FFFFFFFu;   // a word of sentinels / value bits
+    const uint4 sent = make_uint4(sw, sw, sw, sw);
+    for (int i = threadIdx.x; i < n * kVecRow; i += blockDim.x) {
+        const uint4 x = V0[i];
+        uint4 a, b;
+        split_word<TIn>(x.x, sw, &a.x, &b.x);
+        split_word<TIn>(x.y, sw, &a.y, &b.y);
+        split_word<TIn>(x.z, sw, &a.z, &b.z);
+        split_word<TIn>(x.w, sw, &a.w, &b.w);
+        V0[i] = a;
+        V1[i] = b;
+    }
+    for (int i = n * kVecRow + threadIdx.x; i < (rows + kPadRows) * kVecRow; i += blockDim.x) {
+        V0[i] = sent;
+        V1[i] = sent;
+    }
+    for (int i = threadIdx.x; i < kPadRows * kVecRow; i += blockDim.x) {
+        V0[i - kPadRows * kVecRow] = sent;
+        V1[i - kPadRows * kVecRow] = sent;
     }
     __syncthreads();
 

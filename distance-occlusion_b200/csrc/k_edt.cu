@@ -426,22 +426,27 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
                                       : (long long)outer * outer_stride + x;
     // "no cell of the other state reachable": INF (0x7FFF) squared for u16 input, 0x7FFFFFFF for u32
     const uint32_t kNone = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-    for (int qa = 8 * (wi / kGroups) + sub; qa < n; qa += qstep) {
+    const int q0 = 8 * (wi / kGroups) + sub;
+    long long o = base + (long long)q0 * stride;   // output index of the lane's first cell
+    const long long ostep = (long long)qstep * stride, o4 = 4 * stride;
+    for (int qa = q0; qa < n; qa += qstep, o += ostep) {
         const bool has_b = qa + 4 < n;
         const int qb = has_b ? qa + 4 : qa;   // without a second cell the lane walks the first twice
-        const uint32_t sa = F1[qa * TX + col] != 0, sb = F1[qb * TX + col] != 0;   // every own value is >= 1
+        // a cell's value sits in its own state's array, 0 in the other (every own value is >= 1)
+        const uint32_t a0 = F0[qa * TX + col], a1 = F1[qa * TX + col];
+        const uint32_t b0 = F0[qb * TX + col], b1 = F1[qb * TX + col];
+        const uint32_t sa = a1 != 0, sb = b1 != 0;
         const TIn* Aa = (sa ? F1 : F0) + col;
         const TIn* Ab = (sb ? F1 : F0) + col;
-        uint32_t besta = sq_val<TIn>(Aa[qa * TX]), bestb = sq_val<TIn>(Ab[qb * TX]);
+        uint32_t besta = sq_val<TIn>((TIn)(a0 | a1)), bestb = sq_val<TIn>((TIn)(b0 | b1));
         // both sides, two distances per trip, while k^2 < best for either cell
-        // and k stays within kPadRows - 4 of that cell's nearer line end (the
-        // other cell is at most 4 positions away, so neither walks past the
-        // sentinels)
-        const uint32_t kca = (uint32_t)(min(qa, n - 1 - qa) + kPadRows - 4);
-        const uint32_t kcb = (uint32_t)(min(qb, n - 1 - qb) + kPadRows - 4);
-        const uint32_t cap2a = kca * kca, cap2b = kcb * kcb;
+        // and k stays below kcap: within kPadRows - 4 of the nearer line end
+        // of either cell (they are 4 positions apart, so neither walks past
+        // the sentinels)
+        const uint32_t kcap = (uint32_t)(min(qa, n - 1 - qb) + kPadRows - 4);
+        const uint32_t cap2 = kcap * kcap;
         uint32_t k2 = 1, t = 3;   // k^2 and 2k + 1 for the next distance k
-        uint32_t lim = max(min(besta, cap2a), min(bestb, cap2b));
+        uint32_t lim = min(max(besta, bestb), cap2);
         const TIn* pla = Aa + (qa - 1) * TX;
         const TIn* pra = Aa + (qa + 1) * TX;
         const TIn* plb = Ab + (qb - 1) * TX;
@@ -470,16 +475,17 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
             prb += 2 * TX;
             k2 = k2b + t + 2;   // (k+2)^2
             t += 4;
-            lim = max(min(besta, cap2a), min(bestb, cap2b));
+            lim = min(max(besta, bestb), cap2);
         }
-        // a cell whose walk stopped at its cap (more than kPadRows - 4 past its
-        // nearer end) goes on along the far side alone
+        // a cell whose walk stopped at the cap (past its nearer line end: kcap
+        // is at least its distance to that end + kPadRows - 8) goes on along
+        // the far side alone
         const int k = (int)(t >> 1);
         if (k2 < besta) besta = far_side<TIn, TX>(besta, qa, n, k, k2, pla, pra);
-        put_line_value<kFinal>(out, base + (long long)qa * stride, sa, besta >= kNone ? 0xFFFFFFFFu : besta, form);
+        put_line_value<kFinal>(out, o, sa, besta >= kNone ? 0xFFFFFFFFu : besta, form);
         if (has_b) {
             if (k2 < bestb) bestb = far_side<TIn, TX>(bestb, qb, n, k, k2, plb, prb);
-            put_line_value<kFinal>(out, base + (long long)qb * stride, sb, bestb >= kNone ? 0xFFFFFFFFu : bestb, form);
+            put_line_value<kFinal>(out, o + o4, sb, bestb >= kNone ? 0xFFFFFFFFu : bestb, form);
         }
     }
 }

@@ -196,16 +196,77 @@ __device__ __forceinline__ void decode_in(TIn v, uint32_t* state, uint32_t* f)
     }
 }
 
+// sqrtf of the integers 0 .. kSqrtTab - 1 as float bit patterns, built at
+// compile time from an exact integer square root rounded to nearest (no tie
+// is possible: (2m + 1)^2 is odd).  IEEE 754 square root is correctly
+// rounded, so these are the values sqrtf returns; the distances of most cells
+// are below 64, and one cached load replaces the square root there.
+constexpr int kSqrtTab = 4096;
+
+constexpr uint64_t isqrt64(uint64_t n)
+{
+    uint64_t r = 0, bit = 1ull << 62;
+    while (bit > n) bit >>= 2;
+    while (bit) {
+        if (n >= r + bit) {
+            n -= r + bit;
+            r = (r >> 1) + bit;
+        } else {
+            r >>= 1;
+        }
+        bit >>= 2;
+    }
+    return r;   // floor(sqrt(n))
+}
+
+constexpr uint32_t sqrt_bits(uint32_t i)
+{
+    if (i == 0) return 0u;
+    int k = 0;   // i * 4^k in [2^46, 2^48): its square root has 24 bits
+    uint64_t v = i;
+    while (v < (1ull << 46)) {
+        v <<= 2;
+        k++;
+    }
+    uint64_t m = isqrt64(v);
+    if (4 * v > (2 * m + 1) * (2 * m + 1)) m++;   // round to nearest
+    int e = 127 + 23 - k;
+    if (m == (1ull << 24)) {
+        m >>= 1;
+        e++;
+    }
+    return ((uint32_t)e << 23) | (uint32_t)(m - (1ull << 23));
+}
+static_assert(sqrt_bits(4) == 0x40000000u && sqrt_bits(2) == 0x3FB504F3u && sqrt_bits(4095) == 0x427FF800u,
+              "square-root table");
+
+struct SqrtTable {
+    uint32_t v[kSqrtTab];
+};
+constexpr SqrtTable make_sqrt_table()
+{
+    SqrtTable t{};
+    for (int i = 0; i < kSqrtTab; i++) t.v[i] = sqrt_bits((uint32_t)i);
+    return t;
+}
+static __device__ const SqrtTable g_sqrt_table = make_sqrt_table();
+
+// sqrtf((float)e) for an integer squared distance e
+__device__ __forceinline__ float sqrt_of_int(uint32_t e)
+{
+    return e < (uint32_t)kSqrtTab ? __uint_as_float(__ldg(&g_sqrt_table.v[e])) : sqrtf((float)e);
+}
+
 __device__ __forceinline__ float final_value(uint32_t state, uint32_t best, int form)
 {
     // best == 0xFFFFFFFF: no cell of the other state anywhere on the lines searched
-    float e = best == 0xFFFFFFFFu ? FLT_MAX : (float)best;
     if (form == DOL_EDT_SIGNED) {
-        float r = sqrtf(e);
+        const float r = best == 0xFFFFFFFFu ? sqrtf(FLT_MAX) : sqrt_of_int(best);
         return state ? -r : r;
     }
     if (state) return 0.0f;   // unsigned forms: set cells are at distance 0
-    return form == DOL_EDT_DIST ? sqrtf(e) : e;
+    if (best == 0xFFFFFFFFu) return form == DOL_EDT_DIST ? sqrtf(FLT_MAX) : FLT_MAX;
+    return form == DOL_EDT_DIST ? sqrt_of_int(best) : (float)best;
 }
 
 // min over the line of (q-q')^2 + f(q') for the cell at q, walking outwards

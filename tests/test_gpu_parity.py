@@ -152,6 +152,25 @@ def test_edt_mask_forms(dol, O, cuda, dims):
         same_float(host(dol.edt_mask(md, dims, dol.EDT_SIGNED)), O.sdf_signed_felzenszwalb(m, dims))
 
 
+def test_edt_every_small_squared_distance(dol, O, cuda):
+    """One set voxel at the origin of a 64^3 volume: the EDT takes every value
+    x^2 + y^2 + z^2 below 4096 -- every squared distance a volume can give in
+    that range -- so the distances cover every square root the library takes
+    from its table; each must equal the correctly rounded sqrt of the integer."""
+    n = 64
+    b = np.zeros((n, n, n), dtype=bool)
+    b[0, 0, 0] = True
+    md = dev(cuda, O.bool_to_mask(b))
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    sq = (x * x + y * y + z * z).astype(np.int64)
+    want = np.sqrt(sq.astype(np.float32))
+    assert len(np.unique(sq[sq < 4096])) > 3000
+    same_float(host(dol.edt_mask(md, (n, n, n), dol.EDT_DIST)), want)
+    same_float(host(dol.edt_mask(md, (n, n, n), dol.EDT_SQUARED)), sq.astype(np.float32))
+    signed = host(dol.edt_mask(md, (n, n, n), dol.EDT_SIGNED))
+    same_float(signed[1:, :, :], want[1:, :, :])
+
+
 @pytest.mark.parametrize("method", ["danielsson", "fastsweep", "jumpflood"])
 @pytest.mark.parametrize("dims", [(1, 1), (31, 7), (64, 64), (100, 37), (257, 19), (1, 4, 3), (9, 7, 5), (33, 6, 5),
                                   (24, 20, 16)])

@@ -59,6 +59,51 @@ __device__ __forceinline__ int pow2_at_least(int v)
     return p;
 }
 
+// Cells H0 .. H0+15 of a word (me: states, cells past w continuing the last
+// live run; tl / tr: run starts / ends; xb: the word's first cell).  runA is
+// the nearest other-state cell left of cell H0's run; runB comes in as the one
+// right of cell H0+15's run and leaves as the one right of cell H0's.  Each
+// cell's value (distance to the nearer, at most kInf16, state in bit 15)
+// goes out two per word.
+template <int H0>
+__device__ __forceinline__ void x_half(uint32_t me, uint32_t tl, uint32_t tr, int xb, int runA, int& runB,
+                                       uint32_t packed[8])
+{
+    int dl[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int t = H0 + u;
+        if (t > 0 && ((tl >> t) & 1u)) runA = xb + t - 1;
+        dl[u] = xb + t - runA;
+    }
+#pragma unroll
+    for (int u = 15; u >= 0; u--) {
+        const int t = H0 + u;
+        if (t < 31 && ((tr >> t) & 1u)) runB = xb + t + 1;
+        const int d = min(min(dl[u], runB - xb - t), (int)kInf16);
+        const uint32_t v = (uint32_t)d | (((me >> t) & 1u) << 15);
+        if (u & 1)
+            packed[u >> 1] = v << 16;   // the odd cell comes first going down
+        else
+            packed[u >> 1] |= v;
+    }
+}
+
+// 16 cells' packed values to o: two 16-byte stores, or per cell for the first
+// `n` cells when the row end or alignment does not allow them
+__device__ __forceinline__ void store_half(uint16_t* o, const uint32_t pk[8], bool whole, int n)
+{
+    if (whole) {
+        uint4* o4 = reinterpret_cast<uint4*>(o);
+        o4[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        o4[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < 16; t++)
+            if (t < n) o[t] = (uint16_t)(pk[t >> 1] >> (16 * (t & 1)));
+    }
+}
+
 __global__ void __launch_bounds__(256) k_edt_x(const uint32_t* __restrict__ mask, uint16_t* __restrict__ out, int w,
                                                long long rows)
 {
@@ -142,34 +187,19 @@ __global__ void __launch_bounds__(256) k_edt_x(const uint32_t* __restrict__ mask
             const uint32_t tl = me ^ (me << 1);   // bit t: cell t starts a run (t >= 1)
             const uint32_t tr = me ^ (me >> 1);   // bit t: cell t ends a run (t <= 30)
             const int xb = 32 * k;
-            int runA = (me & 1u) ? L0 : L1;       // nearest other-state cell left of the run
-            int dl[32];
-#pragma unroll
-            for (int t = 0; t < 32; t++) {
-                if (t > 0 && ((tl >> t) & 1u)) runA = xb + t - 1;
-                dl[t] = xb + t - runA;
-            }
-            int runB = (me >> 31) ? R0 : R1;      // nearest other-state cell right of the run
-            uint32_t packed[16];
-#pragma unroll
-            for (int t = 31; t >= 0; t--) {
-                if (t < 31 && ((tr >> t) & 1u)) runB = xb + t + 1;
-                const int d = min(min(dl[t], runB - xb - t), (int)kInf16);
-                const uint32_t v = (uint32_t)d | (((me >> t) & 1u) << 15);
-                if (t & 1) packed[t >> 1] = v << 16;
-                else packed[t >> 1] |= v;
-            }
+            // the word in two halves of 16 cells (half the registers of a
+            // whole-word walk): first cells 16..31, whose walk back from the
+            // right carry leaves the value the lower half starts from
+            const int carry_l = (me & 1u) ? L0 : L1;   // nearest other-state cell left of cell 0's run
+            const uint32_t st = tl & 0xFFFEu;          // run starts among cells 1..15
+            int runB = (me >> 31) ? R0 : R1;           // nearest other-state cell right of cell 31's run
+            uint32_t pk[8];
             uint16_t* o = orow + xb;
-            if (vec_ok && nlive == 32) {
-                uint4* o4 = reinterpret_cast<uint4*>(o);
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    o4[j] = make_uint4(packed[4 * j], packed[4 * j + 1], packed[4 * j + 2], packed[4 * j + 3]);
-            } else {
-#pragma unroll
-                for (int t = 0; t < 32; t++)
-                    if (t < nlive) o[t] = (uint16_t)(packed[t >> 1] >> (16 * (t & 1)));
-            }
+            const bool whole = vec_ok && nlive == 32;
+            x_half<16>(me, tl, tr, xb, st ? xb + (30 - __clz(st)) : carry_l, runB, pk);
+            store_half(o + 16, pk, whole, nlive - 16);
+            x_half<0>(me, tl, tr, xb, carry_l, runB, pk);
+            store_half(o, pk, whole, nlive);
         }
     }
 }

@@ -693,7 +693,14 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
     cudaMemsetAsync(flags, 0, (size_t)h * d * sizeof(int), st);
     cudaMemsetAsync(counters, 0, 8 * sizeof(int), st);
 
-    const int s = tuned_s(kTuneFs3, w, 256);
+    // cells per thread: tuned, else rows of at most 128 threads (more CTAs
+    // per SM along the wavefront; 256^3 shapes: 15.1 ms at 128 threads, 22.0
+    // at 256), else at most 256
+    int s = tune_get(kTuneFs3, w);
+    if (!((s == 1 || s == 2 || s == 4 || s == 8) && (w + s - 1) / s <= 256)) {
+        s = pick_s(w, 128);
+        if (!s) s = pick_s(w, 256);
+    }
     const int T = threads_for(w, s);
     ProfScope ps("fastsweep_3d", st);
 #define DOL_FS3_CASE(SV)                                                                                     \

@@ -336,6 +336,29 @@ __device__ __forceinline__ void put_line_value(void* out, long long o, uint32_t 
     }
 }
 
+// A walked cell's result: `none` -- no cell of the other state on the lines
+// searched -- as kInf32 (uint32 field) or the float form's "no cell" value
+template <bool kFinal>
+__device__ __forceinline__ void put_walk_value(void* out, long long o, uint32_t s, uint32_t best, bool none, int form)
+{
+    if (kFinal) {
+        float v;
+        if (form == DOL_EDT_SIGNED) {
+            const float r = none ? sqrtf(FLT_MAX) : sqrt_of_int(best);
+            v = s ? -r : r;
+        } else if (s) {
+            v = 0.0f;   // unsigned forms: set cells are at distance 0
+        } else if (form == DOL_EDT_DIST) {
+            v = none ? sqrtf(FLT_MAX) : sqrt_of_int(best);
+        } else {
+            v = none ? FLT_MAX : (float)best;
+        }
+        static_cast<float*>(out)[o] = v;
+    } else {
+        static_cast<uint32_t*>(out)[o] = (none ? kInf32 : best) | (s << 31);
+    }
+}
+
 // Plain-load form: 32 adjacent x per CTA, the line staged in shared memory when
 // it fits (kStaged) or read from global memory otherwise.
 template <typename TIn, bool kFinal, bool kStaged>
@@ -571,13 +594,13 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         // a cell whose walk stopped at the cap (past its nearer line end: kcap
         // is at least its distance to that end + kPadRows - 8) goes on along
         // the far side alone
-        const int k = (int)(t >> 1);
-        if (k2 < besta) besta = far_side<TIn, TX>(besta, qa, n, k, k2, pla, pra);
-        put_line_value<kFinal>(out, o, sa, besta >= kNone ? 0xFFFFFFFFu : besta, form);
-        if (has_b) {
+        if (k2 < max(besta, bestb)) {   // rare: one test for both cells
+            const int k = (int)(t >> 1);
+            if (k2 < besta) besta = far_side<TIn, TX>(besta, qa, n, k, k2, pla, pra);
             if (k2 < bestb) bestb = far_side<TIn, TX>(bestb, qb, n, k, k2, plb, prb);
-            put_line_value<kFinal>(out, o + o4, sb, bestb >= kNone ? 0xFFFFFFFFu : bestb, form);
         }
+        put_walk_value<kFinal>(out, o, sa, besta, besta >= kNone, form);
+        if (has_b) put_walk_value<kFinal>(out, o + o4, sb, bestb, bestb >= kNone, form);
     }
 }
 

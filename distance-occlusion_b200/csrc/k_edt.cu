@@ -620,6 +620,11 @@ static void line_pass_plain(const TIn* in, void* out, int w, int n, long long st
     }
 }
 
+__global__ void k_flag_error(int* err)
+{
+    atomicExch(err, 2);
+}
+
 // Tensor map of the TMA line kernels: lines along y (along_z = 0) or z of a
 // w x h x d array, TX columns per box row; mode 2: the [y][x/8][z][8] array.
 template <typename TIn, int TX>
@@ -680,7 +685,12 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         return;
     }
     if (mode == 2) {
-        if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 2)) return;
+        if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 2)) {
+            // blocked_layout_ok encoded this map; should the driver refuse it
+            // now, the call reports failure rather than leave the field unwritten
+            k_flag_error<<<1, 1, 0, st>>>(err);
+            return;
+        }
         auto kern = k_edt_line_tma<TIn, kFinal, 8, 2>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
         const unsigned blocks = (unsigned)(outer * (w / 8));

@@ -480,6 +480,9 @@ def _config3(dol, torch, res, L, sp):
         mdv = torch.empty(dol.mask_words(side, side, side), dtype=torch.int32, device="cuda")
         dol.check(L.dol_gen_value_noise_3d(side, side, side, SPACING, C.c_uint32(SEED), C.c_void_p(mdv.data_ptr()), sp))
         dv = torch.empty((side, side, side, 3), dtype=torch.int16, device="cuda")
+        # one untimed run first: its workspace (13.5 GB) comes from the stream-ordered pool
+        dol.init_border(mdv, (side,) * 3, out=dv)
+        dol.danielsson(dv, (side,) * 3, 2)
         dol.init_border(mdv, (side,) * 3, out=dv)
         torch.cuda.synchronize()
         t = _ev_ms(torch, lambda: dol.danielsson(dv, (side,) * 3, 2), 1)

@@ -386,16 +386,18 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
 }
 
 // TMA form.  A TX-column x full-line tile arrives in 256-position boxes
-// (cp.async.bulk.tensor, one mbarrier).  It is then split in place into two
-// state-specific arrays: F_s[p] is the cell's value (v or e) when its state is
-// s and 0 otherwise, so for a cell of state s every probe is one load, one
-// multiply-add (or add) and one min -- a cell of the other state at distance k
-// contributes exactly k^2.  Each array carries kPadRows rows of "no cell"
-// sentinels before and after the line (positions n .. rows-1 too), so the walk
-// outwards from a cell runs on both sides with one test per two distances
-// until it either ends or passes kPadRows beyond the nearer line end; only
-// then does it continue on the far side alone.  A warp covers 8 columns x 4
-// adjacent positions.
+// (cp.async.bulk.tensor, one mbarrier).  It is then split in place, 16 bytes
+// at a time, into two state-specific arrays: F_s[p] is the cell's value (v or
+// e) when its state is s and 0 otherwise, so for a cell of state s every probe
+// is one load and one multiply-add plus a share of a three-way min (uint16
+// distances) or one fused add-min (uint32 squared distances) -- a cell of the
+// other state at distance k contributes exactly k^2.  Each array carries
+// kPadRows rows of "no cell" sentinels before and after the line (positions
+// n .. rows-1 too), so the walk outwards from a cell runs on both sides with
+// one test per two distances until it either ends or passes the nearer line
+// end by the margin the sentinels allow; only then does it continue on the
+// far side alone.  Each lane walks two cells of its column, 4 positions
+// apart, in one loop; a warp covers 8 columns x 8 positions.
 //
 // Layouts (kMode): 0 reads and writes [z][y][x]; 1 (y pass of a volume) writes
 // its uint32 output as [y][x/8][z][8], so that 2 (the z pass) reads every

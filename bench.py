@@ -10,9 +10,11 @@ mask.  Metric: Gvoxels/s of the whole job.  Inputs and outputs (128 MiB mask,
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dol|reference]
 
---impl reference times the reference's own CPU code for the same output on a
-bounded sub-volume (the reference's 1D Felzenszwalb routine applied along z,
-y, x -- it has no 3D driver -- twice, for the two signs, on all host cores).
+--impl reference times the reference's own CPU code for the same output on the
+same 1024^3 volume (the reference's 1D Felzenszwalb routine applied along z,
+y, x -- it has no 3D driver -- twice, for the two signs, then sqrtf and the
+difference, on all host cores); each step is a bounded sample, 1/16 of every
+pass, run with the full volume's strides on the real intermediate fields.
 Under torchrun each rank runs an independent replica (the transform needs the
 whole volume; there is no exchange step), timed on the device, max over ranks.
 """
@@ -133,66 +135,172 @@ def dist_setup():
 
 
 # ---------------------------------------------------------------- reference arm ----
+# The reference's CPU code for the same output: its 1D Felzenszwalb routine
+# (DistanceOcclusionLib.cpp:1026-1062) applied along z, y and x (it has no 3D
+# driver) to the two transforms of the signed field, then sqrtf and the
+# difference.  Only oracle/_ref/libdolref.so (the reference compiled from its
+# own sources) is loaded; the input volume comes from a numpy restatement of
+# the generator, so nothing of this library runs in that arm.
 
-def cpu_reference_sample(side=256, reps=None, target_s=10.0, threads=None):
-    """The reference's CPU code on a side^3 corner of the same noise volume:
-    signed field from two transforms (distance to set, distance to clear) with
-    the reference's 1D Felzenszwalb routine along z, y, x.  Returns Gvox/s."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    dol = load_dol()
-    threads = threads or os.cpu_count() or 1
-    kind = "reference" if O.ref() is not None else "port"
-    n = side
-    # a side^3 volume of the same noise (same spacing, seed and threshold)
-    words = np.zeros(((n + 31) // 32) * n * n, np.uint32)
-    dol.lib().dol_gen_value_noise_3d_host(C.c_int(n), C.c_int(n), C.c_int(n), C.c_int(SPACING), C.c_uint32(SEED),
-                                          words.ctypes.data_as(C.c_void_p))
-    b = O.mask_to_bool(words, (n, n, n))
-    big = np.float32(np.finfo(np.float32).max)
-    done, t0, reps_done = False, time.perf_counter(), 0
-    elapsed = 0.0
-    while not done:
-        t1 = time.perf_counter()
-        f_occ = np.where(b, np.float32(0), big).astype(np.float32)
-        f_emp = np.where(b, big, np.float32(0)).astype(np.float32)
-        if kind == "reference":
-            e_occ = O.felzenszwalb(f_occ, (n, n, n), use_ref=True, threads=threads)
-            e_emp = O.felzenszwalb(f_emp, (n, n, n), use_ref=True, threads=threads)
+REF_FRACTION = 16    # a step transforms 1/16 of every pass's lines (the whole 1024^3 takes ~20 s)
+
+
+def noise_lattice(w, h, d, L, seed):
+    """Lattice values of the value-noise volume: (d//L+2, h//L+2, w//L+2)
+    uint16 from the reference's LCG (DistanceOcclusionLib.cpp:28-32), x fastest."""
+    gx, gy, gz = w // L + 2, h // L + 2, d // L + 2
+    vals = np.empty(gx * gy * gz, np.int64)
+    s = seed & 0xFFFFFFFF
+    for i in range(vals.size):
+        s = (s * 1103515245 + 12345) & 0xFFFFFFFF
+        vals[i] = (s * 65536) >> 32
+    return vals.reshape(gz, gy, gx)
+
+
+def noise_slices(w, h, d, L, seed):
+    """Yields bool[h, w] occupancy per slice z of the value-noise volume: set
+    iff sum(v * wx * wy * wz) over the 8 lattice corners >= 32768 * L^3, the
+    integer form of "trilinear value >= 1/2" (the library's generator)."""
+    lat = noise_lattice(w, h, d, L, seed)
+    xs, ys = np.arange(w), np.arange(h)
+    i, fx = xs // L, xs % L
+    j, fy = ys // L, ys % L
+    wx0, wx1 = (L - fx)[None, :], fx[None, :]
+    wy0, wy1 = (L - fy)[:, None], fy[:, None]
+    thr = 32768 * L ** 3
+    planes = {}
+
+    def plane(k):   # bilinear weights applied within lattice plane k, int64[h, w]
+        if k not in planes:
+            if len(planes) >= 2:
+                del planes[min(planes)]   # slices advance in z: the lowest plane is done
+            v = lat[k]
+            r0 = wx0 * v[np.ix_(j, i)] + wx1 * v[np.ix_(j, i + 1)]
+            r1 = wx0 * v[np.ix_(j + 1, i)] + wx1 * v[np.ix_(j + 1, i + 1)]
+            planes[k] = wy0 * r0 + wy1 * r1
+        return planes[k]
+
+    for z in range(d):
+        k, fz = divmod(z, L)
+        yield ((L - fz) * plane(k) + fz * plane(k + 1)) >= thr
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class ReferenceSample:
+    """Bounded samples of the reference's signed Felzenszwalb on the w x h x d
+    value-noise volume.  Untimed set-up: the volume, the two 0 / FLT_MAX
+    inputs, the full z pass (A) and the y pass of one slab of d/f slices (Y).
+    A timed step then runs, with the full volume's strides and on the real
+    intermediate fields, 1/f of every pass: z lines of w/f columns (raw -> A),
+    the y lines of those columns (A -> A), the x rows of the slab (Y -> X),
+    and sqrtf(occ) - sqrtf(emp) over the slab: 1/f of the whole transform."""
+
+    def __init__(self, w, h, d, fraction=REF_FRACTION, threads=None):
+        self.threads = threads or host_threads()
+        here = os.path.join(ROOT, "oracle")
+        ref_path = os.path.join(here, "_ref", "libdolref.so")
+        if os.path.exists(ref_path):
+            self.kind, self.L = "reference", C.CDLL(ref_path)
+        else:   # the oracle's restatement of the same routine, one thread
+            self.kind, self.L = "port", C.CDLL(os.path.join(here, "liboracle.so"))
+            self.threads = 1
+        self.w, self.h, self.d = w, h, d
+        f = max(1, min(fraction, w, d))
+        self.nx, self.nz = w // f, d // f
+        self.x0, self.z0 = (w - self.nx) // 2, (d - self.nz) // 2
+        self.voxels = self.nx * h * d          # voxels of one pass's sample (equal for all three)
+        self.fraction = w * h * d / self.voxels
+        big = np.float32(np.finfo(np.float32).max)
+        self.raw = [np.empty((d, h, w), np.float32) for _ in range(2)]
+        for z, occ in enumerate(noise_slices(w, h, d, SPACING, SEED)):
+            self.raw[0][z] = np.where(occ, np.float32(0), big)   # transform to set voxels
+            self.raw[1][z] = np.where(occ, big, np.float32(0))   # transform to clear voxels
+        self.A = [np.empty_like(r) for r in self.raw]
+        z0, z1 = self.z0, self.z0 + self.nz
+        for s in range(2):
+            self._pass(self.raw[s], self.A[s], 0, 0, h, 0, w)        # full z pass
+            self._pass(self.A[s], self.A[s], 1, z0, z1, 0, w)        # y pass of the slab
+        self.Y = [np.ascontiguousarray(a[z0:z1]) for a in self.A]
+        self.X = [np.empty_like(y) for y in self.Y]
+        self.out = np.empty_like(self.Y[0])
+        self.sample = (f"1/{self.fraction:.0f} of every pass per step on the {w}x{h}x{d} volume "
+                       f"(z and y lines of x in [{self.x0},{self.x0 + self.nx}), x rows of z in [{z0},{z1})), "
+                       f"both transforms, with the reference's 1D Felzenszwalb (DistanceOcclusionLib.cpp:1026-1062), "
+                       f"then sqrtf difference; {self.threads} host threads")
+
+    def _pass(self, src, dst, pas, a0, a1, b0, b1, dims=None):
+        w, h, d = dims or (self.w, self.h, self.d)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        if self.kind == "reference":
+            self.L.ref_felzenszwalb_3d_pass(w, h, d, vp(src), vp(dst), pas, a0, a1, b0, b1, self.threads)
         else:
-            e_occ = O.felzenszwalb(f_occ, (n, n, n))
-            e_emp = O.felzenszwalb(f_emp, (n, n, n))
-        _ = np.sqrt(e_occ) - np.sqrt(e_emp)
-        elapsed += time.perf_counter() - t1
-        reps_done += 1
-        done = (reps is not None and reps_done >= reps) or (reps is None and time.perf_counter() - t0 >= target_s)
-    vox = reps_done * n ** 3
-    return {"value": vox / elapsed / 1e9, "unit": "Gvoxels/s", "cores": threads if kind == "reference" else 1,
-            "kind": kind,
-            "sample": f"{n}^3 volume of the same noise x{reps_done}: two 3D transforms with the reference's "
-                      f"1D Felzenszwalb (DistanceOcclusionLib.cpp:1026-1062) along z,y,x + sqrt/sub"}
+            n = max(w, h, d)
+            v, zz, line = np.empty(n, np.int32), np.empty(n + 1, np.float32), np.empty(n, np.float32)
+            self.L.dolo_felzenszwalb_3d_pass(w, h, d, vp(src), vp(dst), pas, a0, a1, b0, b1, vp(v), vp(zz), vp(line))
+
+    def step(self):
+        """One timed sample; returns its seconds."""
+        w, h, d = self.w, self.h, self.d
+        xb = (self.x0, self.x0 + self.nx)
+        t = time.perf_counter()
+        for s in range(2):
+            self._pass(self.raw[s], self.A[s], 0, 0, h, *xb)                     # z lines
+        for s in range(2):
+            self._pass(self.A[s], self.A[s], 1, 0, d, *xb)                       # y lines
+        for s in range(2):
+            self._pass(self.Y[s], self.X[s], 2, 0, self.nz, 0, h, (w, h, self.nz))   # x rows
+        n = self.out.size
+        if self.kind == "reference":
+            self.L.ref_sqrt_diff(C.c_longlong(n), self.X[0].ctypes.data_as(C.c_void_p),
+                                 self.X[1].ctypes.data_as(C.c_void_p), self.out.ctypes.data_as(C.c_void_p),
+                                 self.threads)
+        else:
+            np.subtract(np.sqrt(self.X[0]), np.sqrt(self.X[1]), out=self.out)
+        return time.perf_counter() - t
+
+
+def cpu_reference_sample(steps=3, warmup=1):
+    """The reference arm's measurement as the cpu_baseline of a GPU run: a few
+    steps of ReferenceSample on the benchmarked volume.  Returns the
+    cpu_baseline object (Gvox/s of the whole transform)."""
+    rs = ReferenceSample(W, H, D)
+    for _ in range(warmup):
+        rs.step()
+    t = [rs.step() for _ in range(steps)]
+    value = rs.voxels / float(np.mean(t)) / 1e9
+    return {"value": value, "unit": "Gvoxels/s", "cores": rs.threads, "kind": rs.kind,
+            "sample": rs.sample + f"; {steps} timed steps after {warmup} warm-up"}
+
+
+def bench_config(ws):
+    """The benchmarked configuration, identical in both arms."""
+    return {"workload": WORKLOAD, "voxels_per_gpu": W * H * D, "parallelism": f"replicas x{ws}",
+            "l2": "inputs and outputs > L2 (128 MiB mask in, 4 GiB field out); no flush needed"}
 
 
 def run_reference(args):
     ws, rank, local = dist_setup()
     if rank != 0:
         return
-    t_per = []
-    res = None
-    for i in range(args.warmup + args.steps):
-        t = time.perf_counter()
-        res = cpu_reference_sample(side=args.cpu_side, reps=1)
-        if i >= args.warmup:
-            t_per.append(time.perf_counter() - t)
-    vox = args.cpu_side ** 3
-    value = vox / float(np.mean(t_per)) / 1e9
+    rs = ReferenceSample(W, H, D)
+    for _ in range(args.warmup):
+        rs.step()
+    t_per = [rs.step() for _ in range(args.steps)]
+    ms = float(np.mean(t_per)) * 1e3
+    value = rs.voxels / (ms * 1e-3) / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gvoxels/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(t_per)) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"{args.cpu_side}^3 volume of the same noise per step (CPU)"},
-        "cpu_baseline": {"value": value, "unit": "Gvoxels/s", "cores": res["cores"], "kind": res["kind"],
-                         "sample": res["sample"]},
+        "config": bench_config(ws),
+        "cpu_baseline": {"value": value, "unit": "Gvoxels/s", "cores": rs.threads, "kind": rs.kind,
+                         "sample": rs.sample},
         "e2e": {"value": value, "unit": "Gvoxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -614,7 +722,7 @@ def run_dol(args):
                                     for k, v in kern.items()}}
     cpu = None
     if ws == 1 and not args.no_cpu:
-        cpu = cpu_reference_sample(side=args.cpu_side, target_s=args.cpu_seconds)
+        cpu = cpu_reference_sample(steps=args.cpu_steps)
     configs = None
     if not args.no_configs:
         del work
@@ -624,8 +732,7 @@ def run_dol(args):
         "metric": METRIC, "value": value, "unit": "Gvoxels/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (exact integer EDT) -> f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "voxels_per_gpu": W * H * D, "parallelism": f"replicas x{ws}",
-                   "l2": "inputs and outputs > L2 (128 MiB mask in, 4 GiB field out); no flush needed"},
+        "config": bench_config(ws),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "gpu_launches": 3 * args.steps,
         "configs": configs,
@@ -662,8 +769,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dol", choices=["dol", "reference"])
-    ap.add_argument("--cpu-side", type=int, default=256)
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -5,6 +5,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -35,9 +36,11 @@ dol_status fail(dol_status s, const char* fmt, ...)
 }
 
 // Per-device state: SM count and a mapped host word that kernels with bounded
-// waits set when a wait gives up (read by dol_sync).
+// waits set when a wait gives up (read by dol_sync).  `ready` is published
+// with release order after the other fields are written, so a thread that
+// reads it true (acquire) also sees them.
 struct DeviceState {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     int sms = 0;
     int* err_host = nullptr;
     int* err_dev = nullptr;
@@ -53,9 +56,9 @@ dol_status device_state(DeviceState** out)
     if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(DOL_ERR_UNSUPPORTED, "device index %d out of range", dev);
     DeviceState& s = g_dev[dev];
-    if (!s.ready) {
+    if (!s.ready.load(std::memory_order_acquire)) {
         std::lock_guard<std::mutex> lock(g_init_mu);
-        if (!s.ready) {
+        if (!s.ready.load(std::memory_order_relaxed)) {
             int sms = 0;
             e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) return fail(DOL_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
@@ -73,27 +76,12 @@ dol_status device_state(DeviceState** out)
             }
             cudaGetLastError();
             s.sms = sms;
-            s.ready = true;
+            s.ready.store(true, std::memory_order_release);
         }
     }
     g_num_sms = s.sms;
     *out = &s;
     return DOL_OK;
-}
-
-// A pointer the GPU can dereference: device, managed, or mapped host memory.
-dol_status check_dev_ptr(const void* p, const char* name)
-{
-    if (!p) return fail(DOL_ERR_INVALID_ARG, "%s is NULL", name);
-    cudaPointerAttributes a;
-    cudaError_t e = cudaPointerGetAttributes(&a, p);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(DOL_ERR_INVALID_ARG, "%s is not a device pointer (%s)", name, cudaGetErrorString(e));
-    }
-    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return DOL_OK;
-    if (a.type == cudaMemoryTypeHost && a.devicePointer == p) return DOL_OK;
-    return fail(DOL_ERR_INVALID_ARG, "%s is not device-accessible memory", name);
 }
 
 dol_status check_dims(int w, int h, int d)
@@ -134,7 +122,7 @@ dol_status get_workspace(Workspace& ws, void* user, size_t user_bytes, size_t ne
     if (user) {
         if (user_bytes < need)
             return fail(DOL_ERR_INVALID_ARG, "workspace too small: %zu bytes given, %zu needed", user_bytes, need);
-        dol_status s = check_dev_ptr(user, "workspace");
+        dol_status s = (dol_status)check_dev_ptr(user, "workspace");
         if (s != DOL_OK) return s;
         ws.ptr = user;
         return DOL_OK;
@@ -164,7 +152,7 @@ dol_status check_sweep_width(int w)
 
 #define DOL_TRY(x)                          \
     do {                                    \
-        dol_status _s = (x);                \
+        dol_status _s = (dol_status)(x);    \
         if (_s != DOL_OK) return _s;        \
     } while (0)
 
@@ -179,6 +167,21 @@ int dolk::set_error(int s, const char* fmt, ...)
     va_end(ap);
     t_err = buf;
     return s;
+}
+
+// A pointer the GPU can dereference: device, managed, or mapped host memory.
+int dolk::check_dev_ptr(const void* p, const char* name)
+{
+    if (!p) return fail(DOL_ERR_INVALID_ARG, "%s is NULL", name);
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DOL_ERR_INVALID_ARG, "%s is not a device pointer (%s)", name, cudaGetErrorString(e));
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return DOL_OK;
+    if (a.type == cudaMemoryTypeHost && a.devicePointer == p) return DOL_OK;
+    return fail(DOL_ERR_INVALID_ARG, "%s is not device-accessible memory", name);
 }
 
 extern "C" {

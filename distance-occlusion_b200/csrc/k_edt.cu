@@ -606,16 +606,20 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     }
 }
 
+constexpr size_t kStageLimit = 200 * 1024;   // largest staged line tile of the plain form
+
+// set_attr = false: the caller raised the staged kernel's shared-memory limit
+// to kStageLimit beforehand (prepare_edt_mask_2d_plain)
 template <typename TIn, bool kFinal>
 static void line_pass_plain(const TIn* in, void* out, int w, int n, long long stride, long long outer,
-                            long long outer_stride, int form, cudaStream_t st, int outer0 = 0)
+                            long long outer_stride, int form, cudaStream_t st, int outer0 = 0, bool set_attr = true)
 {
     size_t bytes = (size_t)n * 32 * sizeof(TIn);
-    const size_t kStageLimit = 200 * 1024;
     dim3 grid((w + 31) / 32, (unsigned)outer);
     if (bytes <= kStageLimit) {
         auto kern = k_edt_line<TIn, kFinal, true>;
-        if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (set_attr && bytes > 48 * 1024)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         kern<<<grid, 256, bytes, st>>>(in, out, w, n, stride, outer_stride, form, outer0);
     } else {
         k_edt_line<TIn, kFinal, false><<<grid, 256, 0, st>>>(in, out, w, n, stride, outer_stride, form, outer0);
@@ -810,14 +814,21 @@ void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, 
 }
 
 // 2D mask EDT on caller-provided scratch (w*h uint16), plain loads only: no
-// tensor maps, no bounded waits, nothing allocated.
+// tensor maps, no bounded waits, nothing allocated.  The staged column
+// kernel's shared-memory limit comes from prepare_edt_mask_2d_plain.
 void launch_edt_mask_2d_plain(const uint32_t* mask, float* out, int w, int h, int form, uint16_t* scratch, int sms,
                               cudaStream_t st)
 {
     long long blocks = ((long long)h * 32 + 255) / 256;
     long long cap = (long long)sms * 16;
     k_edt_x<<<(int)(blocks < cap ? blocks : cap), 256, 0, st>>>(mask, scratch, w, h);
-    line_pass_plain<uint16_t, true>(scratch, out, w, h, w, 1, 0, form, st);
+    line_pass_plain<uint16_t, true>(scratch, out, w, h, w, 1, 0, form, st, 0, false);
+}
+
+cudaError_t prepare_edt_mask_2d_plain()
+{
+    return cudaFuncSetAttribute(k_edt_line<uint16_t, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kStageLimit);
 }
 
 // ------------------------------------------------ faithful float Felzenszwalb ----

@@ -15,6 +15,11 @@
 // later reads, so nothing needs clearing.  Calls that overlap on the GPU
 // (different streams, or different host threads on one device) race on the
 // array: serialise them.
+//
+// The first call on a device does that device's set-up (the array's device
+// address, the SM count, the column kernel's shared-memory limit); make that
+// first call before capturing any stream into a CUDA graph.
+#include <atomic>
 #include <mutex>
 
 #include "dol_b200.h"
@@ -25,8 +30,10 @@ namespace dolk {
 constexpr size_t kNoAllocMaxCells = (size_t)8 << 20;   // 8,388,608 cells, e.g. 2896 x 2896 or 4096 x 2048
 static __device__ __align__(256) uint16_t g_edt2_scratch[kNoAllocMaxCells];
 
+// `ready` is stored (release) after scratch and sms are written; a caller
+// that loads it true (acquire) sees both
 struct NoAllocDevice {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     uint16_t* scratch = nullptr;   // device address of g_edt2_scratch on this device
     int sms = 0;
 };
@@ -50,16 +57,8 @@ extern "C" DOL_API dol_status dol_edt_mask_2d_noalloc(int w, int h, const uint32
                                      w, h, (size_t)w * h, kNoAllocMaxCells);
     if (form != DOL_EDT_SQUARED && form != DOL_EDT_DIST && form != DOL_EDT_SIGNED)
         return (dol_status)set_error(DOL_ERR_INVALID_ARG, "form must be DOL_EDT_SQUARED, DOL_EDT_DIST or DOL_EDT_SIGNED");
-    const void* ptrs[2] = {mask, out};
-    const char* names[2] = {"mask", "out"};
-    for (int i = 0; i < 2; i++) {
-        cudaPointerAttributes a;
-        if (!ptrs[i] || cudaPointerGetAttributes(&a, ptrs[i]) != cudaSuccess ||
-            (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)) {
-            cudaGetLastError();
-            return (dol_status)set_error(DOL_ERR_INVALID_ARG, "%s is not device memory", names[i]);
-        }
-    }
+    if (check_dev_ptr(mask, "mask") != DOL_OK) return DOL_ERR_INVALID_ARG;
+    if (check_dev_ptr(out, "out") != DOL_OK) return DOL_ERR_INVALID_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
@@ -68,9 +67,9 @@ extern "C" DOL_API dol_status dol_edt_mask_2d_noalloc(int w, int h, const uint32
     // set-up, once per device, with that device current: the array's name is
     // only a host-side stand-in; the kernels need its device address
     NoAllocDevice& nd = g_noalloc[dev];
-    if (!nd.ready) {
+    if (!nd.ready.load(std::memory_order_acquire)) {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!nd.ready) {
+        if (!nd.ready.load(std::memory_order_relaxed)) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_edt2_scratch);
             if (e != cudaSuccess) {
@@ -83,11 +82,18 @@ extern "C" DOL_API dol_status dol_edt_mask_2d_noalloc(int w, int h, const uint32
                 cudaGetLastError();
                 return (dol_status)set_error(DOL_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
             }
+            e = prepare_edt_mask_2d_plain();
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return (dol_status)set_error(DOL_ERR_CUDA, "cudaFuncSetAttribute (column kernel): %s",
+                                             cudaGetErrorString(e));
+            }
             nd.scratch = static_cast<uint16_t*>(p);
             nd.sms = sms;
-            nd.ready = true;
+            nd.ready.store(true, std::memory_order_release);
         }
     }
+    cudaGetLastError();   // an earlier asynchronous error is not this call's
     launch_edt_mask_2d_plain(mask, out, w, h, form, nd.scratch, nd.sms, static_cast<cudaStream_t>(stream));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (dol_status)set_error(DOL_ERR_CUDA, "edt_mask_2d_noalloc: %s", cudaGetErrorString(e));

@@ -23,6 +23,9 @@ private:
 
 // records the message returned by dol_last_error() and returns `s`
 int set_error(int s, const char* fmt, ...);
+// DOL_OK (0) for a pointer the GPU can dereference (device, managed or mapped
+// host memory), else DOL_ERR_INVALID_ARG with the message recorded
+int check_dev_ptr(const void* p, const char* name);
 
 // launch-configuration table (tune.cu); values are family specific, 0 = use
 // the launcher's heuristic.  The order matches the DOL_TUNE_* constants.
@@ -66,6 +69,8 @@ void launch_edt_mask_3d_chunked(const uint32_t* mask, float* out, int w, int h, 
                                 void (*done)(void*, int, int), void* ctx);
 void launch_edt_mask_2d_plain(const uint32_t* mask, float* out, int w, int h, int form, uint16_t* scratch, int sms,
                               cudaStream_t st);
+// the kernel attributes launch_edt_mask_2d_plain relies on (set once per device)
+cudaError_t prepare_edt_mask_2d_plain();
 // faithful float Felzenszwalb (2D, arbitrary input)
 size_t felz_float_workspace_bytes(int w, int h);
 void launch_felz_float_2d(float* dist, int w, int h, void* ws, cudaStream_t st);

@@ -11,8 +11,8 @@
 // no error reporting; it would crash or write out of bounds instead).
 //
 // The occlusion routines of the reference (InitDirWFromBitMask,
-// OcclusionSweep, ShadowSweep, Encode*) and Chamfer are not provided here:
-// they stay with the reference library on the host.
+// OcclusionSweep, ShadowSweep, Encode*) are not provided here: they stay with
+// the reference library on the host.
 #ifndef DISTANCE_OCCLUSION_B200_H
 #define DISTANCE_OCCLUSION_B200_H
 

@@ -861,6 +861,25 @@ void dolo_felzenszwalb_3d(int w, int h, int d, float* dist, float* td, int* v, f
         }
 }
 
+/* One pass of the 3D restatement over a rectangle of its lines (a0 <= a < a1,
+ * b0 <= b < b1): pass 0 z lines (a = y, b = x), 1 y lines (a = z, b = x), 2 x
+ * rows (a = z, b = y); src -> dst, both whole volumes (dst may be src).  v, z
+ * and line are scratch for one line (max(w,h,d) ints, one more float, and
+ * max(w,h,d) floats). */
+void dolo_felzenszwalb_3d_pass(int w, int h, int d, const float* src, float* dst, int pass, int a0, int a1, int b0,
+                               int b1, int* v, float* z, float* line)
+{
+    size_t ss = (size_t)w * h;
+    int n = pass == 0 ? d : (pass == 1 ? h : w);
+    size_t stride = pass == 0 ? ss : (pass == 1 ? (size_t)w : 1);
+    for (int a = a0; a < a1; a++)
+        for (int b = b0; b < b1; b++) {
+            size_t base = pass == 0 ? (size_t)a * w + b : (pass == 1 ? (size_t)a * ss + b : (size_t)a * ss + (size_t)b * w);
+            felz_line(n, (int)stride, src + base, line, v, z);
+            for (int q = 0; q < n; q++) dst[base + (size_t)q * stride] = line[q];
+        }
+}
+
 /* ---- deltas -> distances ------------------------------------------------- */
 
 void dolo_deltas_to_dist_2d(int w, int h, const i16* deltas, int cw, const uint32_t* sign_mask, float* out)

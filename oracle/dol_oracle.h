@@ -72,6 +72,10 @@ void dolo_bruteforce_3d(int w, int h, int d, int16_t* deltas, int cw, int exact)
    then y, then x. */
 void dolo_felzenszwalb_2d(int w, int h, float* dist, float* td, int* v, float* z);
 void dolo_felzenszwalb_3d(int w, int h, int d, float* dist, float* td, int* v, float* z);
+/* one pass of the 3D form over lines (a, b), a0 <= a < a1, b0 <= b < b1 (pass 0:
+   z lines, a = y, b = x; 1: y lines, a = z, b = x; 2: x rows, a = z, b = y) */
+void dolo_felzenszwalb_3d_pass(int w, int h, int d, const float* src, float* dst, int pass, int a0, int a1, int b0,
+                               int b1, int* v, float* z, float* line);
 
 /* deltas -> float distances (DistanceOcclusionTool.cpp:46-61, sign as at
    :1262/:1392): sqrtf((float)len2) / cw, negated where sign_mask has the bit */

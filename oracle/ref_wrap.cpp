@@ -86,4 +86,59 @@ void ref_felzenszwalb_3d(int w, int h, int d, float* dist, int threads)
     }
 }
 
+/* One pass of the same 3D restatement over a rectangle of its lines, for
+ * timing bounded samples of a large volume.  pass 0: z lines (a = y, b = x);
+ * 1: y lines (a = z, b = x); 2: x rows (a = z, b = y); lines (a, b) with
+ * a0 <= a < a1, b0 <= b < b1.  Reads src, writes dst (both whole w*h*d
+ * volumes, so strides are those of the full volume; dst may be src: every
+ * line goes through a private buffer).  Each of `threads` host threads takes
+ * one contiguous block of the lines in (a, b) order, as a static loop
+ * schedule would. */
+void ref_felzenszwalb_3d_pass(int w, int h, int d, const float* src, float* dst, int pass, int a0, int a1, int b0,
+                              int b1, int threads)
+{
+    if (threads < 1) threads = 1;
+    const size_t ss = (size_t)w * h;
+    const int n = pass == 0 ? d : (pass == 1 ? h : w);
+    const size_t stride = pass == 0 ? ss : (pass == 1 ? (size_t)w : 1);
+    const long long nb = b1 - b0, lines = (long long)(a1 - a0) * nb;
+    auto line_base = [&](long long i) -> size_t {
+        const size_t a = (size_t)(a0 + i / nb), b = (size_t)(b0 + i % nb);
+        if (pass == 0) return a * w + b;         /* (y, x): column through all slices */
+        if (pass == 1) return a * ss + b;        /* (z, x): column of slice z */
+        return a * ss + b * w;                   /* (z, y): row */
+    };
+    auto run = [&](int t) {
+        std::vector<int> v(n);
+        std::vector<float> z(n + 1), line(n);
+        const long long lo = lines * t / threads, hi = lines * (t + 1) / threads;
+        for (long long i = lo; i < hi; i++) {
+            const size_t base = line_base(i);
+            ::Felzenszwalb(n, (int)stride, src + base, line.data(), v.data(), z.data());
+            float* o = dst + base;
+            for (int q = 0; q < n; q++) o[(size_t)q * stride] = line[q];
+        }
+    };
+    if (threads == 1) { run(0); return; }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) pool.emplace_back(run, t);
+    for (auto& th : pool) th.join();
+}
+
+/* The signed field from the two squared transforms, as the tool's two-pass
+ * path forms it (DistanceOcclusionTool.cpp:54-61, :1036): out = sqrtf(occ) -
+ * sqrtf(emp), over n floats split across `threads` host threads. */
+void ref_sqrt_diff(long long n, const float* occ, const float* emp, float* out, int threads)
+{
+    if (threads < 1) threads = 1;
+    auto run = [&](int t) {
+        const long long lo = n * t / threads, hi = n * (t + 1) / threads;
+        for (long long i = lo; i < hi; i++) out[i] = sqrtf(occ[i]) - sqrtf(emp[i]);
+    };
+    if (threads == 1) { run(0); return; }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) pool.emplace_back(run, t);
+    for (auto& th : pool) th.join();
+}
+
 }  /* extern "C" */

@@ -7,7 +7,9 @@
    the row padding bits.
 3. Against the reference's README images (images/*-sdf.png regenerated from
    data/*.png), which reproduce within +-1 grey level -- a weak check, run only
-   where the reference checkout exists.
+   where the reference checkout exists: the directory in DOL_REFERENCE_DIR, or
+   the one oracle/Makefile recorded in oracle/_ref/ref_dir.txt when it built
+   the reference.
 """
 import hashlib
 import json
@@ -18,7 +20,21 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
-REF_DIR = "/root/reference"
+
+
+def _reference_dir():
+    """The reference checkout: DOL_REFERENCE_DIR, else the directory the oracle
+    recipe built oracle/_ref from; None when neither names an existing one."""
+    d = os.environ.get("DOL_REFERENCE_DIR")
+    if not d:
+        rec = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "ref_dir.txt")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                d = f.read().strip()
+    return d if d and os.path.isdir(d) else None
+
+
+REF_DIR = _reference_dir()
 
 
 def digest(a):
@@ -251,8 +267,8 @@ def _readme_case(O, name):
 
 @pytest.mark.parametrize("name", ["tiger", "kiwi"])
 def test_readme_sdf_images_within_one_level(O, name):
-    if not os.path.isdir(REF_DIR):
-        pytest.skip("reference checkout not present")
+    if REF_DIR is None:
+        pytest.skip("reference checkout not present (set DOL_REFERENCE_DIR)")
     enc, want = _readme_case(O, name)
     diff = np.abs(enc - want)
     assert diff.max() <= 1, f"max grey-level difference {diff.max()}"

@@ -33,7 +33,11 @@ def _call(dol, torch, mask, dims, form):
 def test_no_alloc_edt_matches_allocating_entry_point(dol, O, cuda):
     torch = cuda
     rng = np.random.default_rng(2024)
-    cases = [((700, 500), 0.02, dol.EDT_SIGNED), ((333, 129), 0.3, dol.EDT_DIST), ((2048, 1024), 0.001, dol.EDT_SQUARED)]
+    # columns of up to 3200 cells are staged in shared memory, taller ones are
+    # read from global memory: 1024 x 4096 takes the second branch, and
+    # 4096 x 2048 is exactly the array's 8,388,608-cell limit
+    cases = [((700, 500), 0.02, dol.EDT_SIGNED), ((333, 129), 0.3, dol.EDT_DIST), ((2048, 1024), 0.001, dol.EDT_SQUARED),
+             ((1024, 4096), 0.0005, dol.EDT_SIGNED), ((4096, 2048), 0.0002, dol.EDT_DIST)]
     for dims, p, form in cases:
         w, h = dims
         m = O.bool_to_mask(rng.random((h, w)) < p)

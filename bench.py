@@ -353,6 +353,8 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
         _config5(dol, torch, res)
     if big and want("c3"):
         _config3(dol, torch, res, L, sp)
+    if want("c7"):
+        _config_sparse(dol, torch, O, ref, res, L, sp, big)
     if only is not None and "c6" in only:
         _sweep_variants(dol, torch, res, L, sp, big)
     return res
@@ -601,6 +603,60 @@ def _config3(dol, torch, res, L, sp):
         del dv, mdv
 
 
+def _config_sparse(dol, torch, O, ref, res, L, sp, big=True):
+    """The mask EDT where the nearest cell of the other state can be far away:
+    the 2D default image (1024^2, 100 points, seed 1) through the mask EDT and
+    through the tool's float path (InitDistancesFromBitMask + Felzenszwalb,
+    DistanceOcclusionTool.cpp:741-782), and 1024^3 volumes of 2000 points
+    (BitMaskAddPoints, seed 1) and of no set voxel, signed."""
+    out = {}
+    dims = (1024, 1024)
+    m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+    md = torch.from_numpy(m.view(np.int32)).cuda()
+    f2 = dol.empty_field(dims)
+    ws2 = torch.empty(L.dol_edt_mask_2d_workspace_size(*dims), dtype=torch.uint8, device="cuda")
+    run = lambda: dol.edt_mask(md, dims, dol.EDT_DIST, out=f2, workspace=ws2)
+    run()
+    out["edt_2d_1024_points100_ms"] = _ev_ms(torch, run, 5)
+    f0 = dol.init_distances(md, dims)
+    wf = torch.empty(L.dol_felzenszwalb_2d_workspace_size(*dims), dtype=torch.uint8, device="cuda")
+    ff = f0.clone()
+
+    def run_f():
+        ff.copy_(f0)
+        dol.check(L.dol_felzenszwalb_2d(1024, 1024, C.c_void_p(ff.data_ptr()), C.c_void_p(wf.data_ptr()),
+                                        C.c_size_t(wf.numel()), sp))
+    run_f()
+    out["felzenszwalb_float_2d_1024_points100_ms"] = _ev_ms(torch, run_f, 3) - _ev_ms(torch, lambda: ff.copy_(f0), 3)
+    if ref is not None:
+        fi = O.init_distances(m, dims, use_ref=True)
+        t0 = time.perf_counter()
+        O.felzenszwalb(fi, dims, use_ref=True)
+        out["cpu_ref_felzenszwalb_2d_1024_points100_ms"] = (time.perf_counter() - t0) * 1e3
+    if big:
+        side = 1024
+        d3 = (side,) * 3
+        mh = np.zeros(dol.mask_words(*d3), np.uint32)
+        cases = {"points2000": dol.add_points(mh.copy(), d3, 2000, 1), "empty": mh}
+        f3 = dol.empty_field(d3)
+        ws3 = torch.empty(L.dol_edt_mask_3d_workspace_size(*d3), dtype=torch.uint8, device="cuda")
+        for name, mk in cases.items():
+            mdv = torch.from_numpy(mk.view(np.int32)).cuda()
+            run3 = lambda: dol.edt_mask(mdv, d3, dol.EDT_SIGNED, out=f3, workspace=ws3)
+            run3()
+            torch.cuda.synchronize()
+            L.dol_profile_begin()
+            t = _ev_ms(torch, run3, 1)
+            names_buf = C.create_string_buffer(4096)
+            ms = (C.c_float * 64)()
+            n = L.dol_profile_end(names_buf, C.c_size_t(4096), ms, C.c_int(64))
+            per = dict(zip(names_buf.value.decode().split("\n")[:n], list(ms)[:n]))
+            out[f"edt_3d_1024_{name}_ms"] = t
+            out[f"edt_3d_1024_{name}_per_kernel_ms"] = per
+        del f3, ws3
+    res["edt_sparse"] = out
+
+
 def _batch_item_type():
     class Item(C.Structure):
         _fields_ = [("w", C.c_int), ("h", C.c_int), ("d", C.c_int), ("reserved", C.c_int),
@@ -778,7 +834,7 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration measurements")
     ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
     ap.add_argument("--only", default=None,
-                    help="comma list of c1..c6: run only these per-configuration measurements (no headline)")
+                    help="comma list of c1..c7: run only these per-configuration measurements (no headline)")
     ap.add_argument("--danielsson", default=None, metavar="WxHxD",
                     help="only time signed Danielsson on a WxHxD value-noise volume (twice; for profiling)")
     args = ap.parse_args()

@@ -27,6 +27,7 @@
 #include <float.h>
 
 #include "common.cuh"
+#include "hull.cuh"
 #include "kernels.h"
 #include "tma.cuh"
 
@@ -404,11 +405,6 @@ __global__ void __launch_bounds__(256) k_edt_line(const TIn* __restrict__ in, vo
 // 8-column z line as one contiguous 32-byte-row tile.
 constexpr int kPadRows = 32;
 
-template <typename TIn>
-__device__ __forceinline__ uint32_t sq_val(TIn v)
-{
-    return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v : (uint32_t)v;
-}
 // sq_val(v) + k2: one multiply-add for the u16 (distance) form
 template <typename TIn>
 __device__ __forceinline__ uint32_t add_sq(TIn v, uint32_t k2)
@@ -439,10 +435,13 @@ __device__ __forceinline__ uint32_t far_side(uint32_t best, int q, int n, int k,
     return best;
 }
 
+// the two split line arrays with their sentinel rows, then the envelope
+// path's hull words (two per column per 32-cell segment)
 template <typename TIn, int TX>
 static size_t tma_tile_bytes(int n)
 {
-    return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn);
+    return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn) +
+           2 * (size_t)TX * ((n + 31) / 32) * sizeof(uint32_t);
 }
 
 // One 32-bit word of a staged tile split by state: its cells (two uint16 or
@@ -458,10 +457,16 @@ __device__ __forceinline__ void split_word(uint32_t x, uint32_t vmask, uint32_t*
     *f1 = v & m;
 }
 
+// Envelope path (hull.cuh): the windowed search costs a cell about sqrt(its
+// own value) probes, and a cell with no cell of the other state on its row
+// (or plane) walks to the line end, so sparse or nearly empty volumes make it
+// O(n) per cell.  Tiles holding such values take the lower-envelope path,
+// O(n) per line whatever the data.
+
 template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
-                                                      int along_z, int form, int* err, int outer0)
+                                                      int along_z, int form, int* err, int outer0, uint32_t hull_thr)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
@@ -507,6 +512,14 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     uint4* V1 = reinterpret_cast<uint4*>(F1);
     const uint32_t sw = sizeof(TIn) == 2 ? 0x7FFF7FFFu : 0x7FFFFFFFu;   // a word of sentinels / value bits
     const uint4 sent = make_uint4(sw, sw, sw, sw);
+    // while splitting, note any own value above the window threshold (a
+    // distance above hull_thr; "none" counts): such a tile takes the envelope path
+    const uint32_t thr = sizeof(TIn) == 2 ? (hull_thr > 0x7FFFu ? 0x7FFFu : hull_thr) * 0x00010001u
+                                          : (hull_thr >= 46341u ? 0x7FFFFFFFu : hull_thr * hull_thr);
+    uint32_t big = 0;
+    auto over = [&](uint32_t x) -> uint32_t {
+        return sizeof(TIn) == 2 ? __vcmpgtu2(x & sw, thr) : (uint32_t)((x & sw) > thr);
+    };
     for (int i = threadIdx.x; i < n * kVecRow; i += blockDim.x) {
         const uint4 x = V0[i];
         uint4 a, b;
@@ -516,6 +529,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         split_word<TIn>(x.w, sw, &a.w, &b.w);
         V0[i] = a;
         V1[i] = b;
+        big |= over(x.x) | over(x.y) | over(x.z) | over(x.w);
     }
     for (int i = n * kVecRow + threadIdx.x; i < (rows + kPadRows) * kVecRow; i += blockDim.x) {
         V0[i] = sent;
@@ -525,7 +539,43 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         V0[i - kPadRows * kVecRow] = sent;
         V1[i - kPadRows * kVecRow] = sent;
     }
-    __syncthreads();
+    const bool use_hull = __syncthreads_or(big != 0 && hull_thr != 0xFFFFFFFFu);
+
+    if (use_hull) {
+        // envelope path: units (column, 32-cell segment); hull words after the tile
+        const int nseg = (n + 31) >> 5;
+        uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
+        const int units = TX * nseg;
+        for (int u = threadIdx.x; u < units; u += blockDim.x) {
+            const int col = u % TX, seg = u / TX;
+            if (x0 + col < w) hull_build<TIn>(F0, F1, HM, TX, nseg, n, col, seg);
+        }
+        __syncthreads();
+        for (int half = 1; half < nseg; half <<= 1) {
+            const int groups = (nseg + 2 * half - 1) / (2 * half);
+            for (int j = threadIdx.x; j < 2 * TX * groups; j += blockDim.x) {
+                const int g = j % groups, sc = j / groups;   // sc = s * TX + col
+                const int col = sc % TX, s = sc / TX;
+                const int lo = g * 2 * half, mid = lo + half, hi = min(mid + half, nseg);
+                if (mid < nseg && x0 + col < w)
+                    hull_merge<TIn>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
+            }
+            __syncthreads();
+        }
+        const uint32_t kNoneH = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
+        for (int u = threadIdx.x; u < units; u += blockDim.x) {
+            const int col = u % TX, seg = u / TX;
+            const int x = x0 + col;
+            if (x >= w) continue;
+            const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
+                                              : (long long)outer * outer_stride + x;
+            hull_query<TIn>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
+                put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best, none || best >= kNoneH,
+                                       form);
+            });
+        }
+        return;
+    }
 
     // a warp covers 8 columns x 8 positions, each lane two cells of its
     // column 4 apart, both walked in one loop (a compact footprint:
@@ -662,6 +712,18 @@ static bool blocked_layout_ok(const uint16_t* vx, const uint32_t* ey, int w, int
     return line_map<uint16_t, 16>(&m, vx, w, h, d, 0, 1) && line_map<uint32_t, 8>(&m, ey, w, h, d, 1, 2);
 }
 
+// Window threshold of the line passes: a tile holding an own value (a cell's
+// distance to the other state in the lower dimensions) above it takes the
+// envelope path.  The tuned value (DOL_TUNE_EDT_HULL, by line length): 1 =
+// windowed search only, 2 = envelope only, >= 3 = that distance; 0 = 24.
+static uint32_t edt_hull_threshold(int n)
+{
+    const int v = tune_get(kTuneEdtHull, n);
+    if (v == 1) return 0xFFFFFFFFu;
+    if (v == 2) return 0u;
+    return v >= 3 ? (uint32_t)v : 24u;
+}
+
 // Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
 // of a w x h x d array; outer indices outer0 .. outer0 + nouter - 1 (nouter < 0:
 // all).  TMA needs 16-byte row pitches and a tile that fits in shared memory;
@@ -681,13 +743,14 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
     const int tv = tune_get(kTuneEdt, w);
     const int threads = tv == 256 ? 256 : 512;
+    const uint32_t hthr = edt_hull_threshold(n);
     CUtensorMap map;
     if (mode == 1) {
         if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) return;   // blocked_layout_ok encoded it already
         auto kern = k_edt_line_tma<TIn, kFinal, TX, 1>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
         dim3 grid((w + TX - 1) / TX, (unsigned)outer);
-        kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0);
+        kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0, hthr);
         return;
     }
     if (mode == 2) {
@@ -700,7 +763,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         auto kern = k_edt_line_tma<TIn, kFinal, 8, 2>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
         const unsigned blocks = (unsigned)(outer * (w / 8));
-        kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0);
+        kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0, hthr);
         return;
     }
     if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {
@@ -708,7 +771,8 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
             auto kern = k_edt_line_tma<TIn, kFinal, TX, 0>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
-            kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0);
+            kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0,
+                                                    hthr);
             return;
         }
     }

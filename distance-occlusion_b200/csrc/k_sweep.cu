@@ -15,6 +15,8 @@
 // atomic counter and wait (bounded) on per-row ready flags.  A row is only
 // claimed by a running CTA and every row it waits on was claimed earlier, so
 // the earliest unfinished row can always proceed.
+#include <limits.h>
+
 #include "kernels.h"
 #include "scan.cuh"
 
@@ -287,7 +289,7 @@ template <int S>
 __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, int w, int h, int d, int cw, int sweep,
                                                     int* __restrict__ flags, int* __restrict__ counter,
                                                     const int* __restrict__ diag_start, int* __restrict__ err,
-                                                    int epoch)
+                                                    int epoch, int wait_epoch, unsigned wait_limit)
 {
     __shared__ ScanShared<C3> sh;
     __shared__ int s_item;
@@ -330,10 +332,12 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
             // wait (bounded) until both neighbour rows of this sweep are done
             const int* fa = jj > 1 ? flags + (long long)z * h + yprev : nullptr;
             const int* fb = kk > 1 ? flags + (long long)zprev * h + y : nullptr;
-            for (int it = 0;; it++) {
-                bool ok = (!fa || *((volatile const int*)fa) >= epoch) && (!fb || *((volatile const int*)fb) >= epoch);
+            // (wait_epoch is epoch except under a test hook that makes it unreachable)
+            for (unsigned it = 0;; it++) {
+                bool ok = (!fa || *((volatile const int*)fa) >= wait_epoch) &&
+                          (!fb || *((volatile const int*)fb) >= wait_epoch);
                 if (ok) break;
-                if (it > (1 << 22)) { atomicExch(err, 1); break; }
+                if (it >= wait_limit) { atomicExch(err, 1); break; }
                 __nanosleep(128);
             }
             __threadfence();
@@ -702,6 +706,7 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
         if (!s) s = pick_s(w, 256);
     }
     const int T = threads_for(w, s);
+    const WaitHooks hooks = wait_hooks();
     ProfScope ps("fastsweep_3d", st);
 #define DOL_FS3_CASE(SV)                                                                                     \
     case SV: {                                                                                               \
@@ -713,7 +718,9 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
         if (grid > rows) grid = rows;                                                                        \
         for (int sw = 0; sw < 8; sw++)                                                                       \
             k_fastsweep3<SV><<<(int)grid, T, 0, st>>>(static_cast<int16_t*>(deltas), w, h, d, cw, sw, flags,  \
-                                                      counters + sw, diag, err, sw + 1);                     \
+                                                      counters + sw, diag, err, sw + 1,                       \
+                                                      sw == hooks.stall_sweep ? INT_MAX : sw + 1,             \
+                                                      hooks.limit);                                           \
     } break;
     switch (s) {
         DOL_FS3_CASE(1)

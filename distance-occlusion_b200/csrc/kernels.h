@@ -40,10 +40,22 @@ enum TuneKind {
     kTuneEdt,
     kTuneDanRows,
     kTuneDanSlices,
+    kTuneEdtHull,
     kTuneKinds
 };
 int tune_get(int kind, int w);
 void tune_put(int kind, int w, int value);
+
+// Test hooks of the bounded device waits (dol_test_wait_hooks): the 3D
+// FastSweep row wait gives up after `limit` polls (~128 ns apart); when
+// stall_sweep is 0..7 that sweep's rows wait for a flag value no row ever
+// writes, so every wait with a predecessor runs out.  Defaults: no stall,
+// 2^22 polls.
+struct WaitHooks {
+    int stall_sweep;
+    unsigned limit;
+};
+WaitHooks wait_hooks();
 
 inline uint32_t float_bits(float f)
 {

@@ -56,6 +56,15 @@ void tune_put(int kind, int w, int value)
     g_tune[cur_dev()][kind][bucket_of(w)] = value;
 }
 
+// test hooks of the bounded waits (kernels.h); process-wide, read at launch
+static WaitHooks g_wait_hooks = {-1, 1u << 22};
+
+WaitHooks wait_hooks()
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    return g_wait_hooks;
+}
+
 // candidate values per family
 static std::vector<int> candidates(int kind, int w)
 {
@@ -146,6 +155,13 @@ static dol_status tune_batch(cudaStream_t st)
 extern "C" {
 
 DOL_API int dol_tune_get(int kind, int w) { return tune_get(kind, w); }
+
+DOL_API void dol_test_wait_hooks(int stall_sweep, unsigned limit)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_wait_hooks.stall_sweep = stall_sweep >= 0 && stall_sweep < 8 ? stall_sweep : -1;
+    g_wait_hooks.limit = limit ? limit : 1u << 22;
+}
 
 DOL_API void dol_tune_set(int kind, int w, int value) { tune_put(kind, w, value); }
 

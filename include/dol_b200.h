@@ -284,9 +284,25 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_DANIELSSON_ROWS 8 /* Danielsson block schedule: rows per block (1..4096);
                                       65536 = the serial single-CTA engine */
 #define DOL_TUNE_DANIELSSON_SLICES 9 /* Danielsson block schedule: slices per block (3D) */
+#define DOL_TUNE_EDT_HULL     10   /* EDT line passes, by line length: a tile whose cells lie farther than this
+                                      from the other state along the lower dimensions takes the lower-envelope
+                                      path instead of the windowed search; 1 = window only, 2 = envelope only */
 DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream);
 DOL_API int        dol_tune_get(int kind, int w);
 DOL_API void       dol_tune_set(int kind, int w, int value);
+
+/* ---- failure-detection test hook (no reference counterpart; the reference
+   has no error reporting, DistanceOcclusionLib.cpp:14-18 asserts only) ---------------
+   For tests of the timeout path only; process-wide, affects later launches.
+   The 3D FastSweep wavefront (dol_fastsweep_3d, dol_sdf_3d with FastSweep)
+   waits, per row, for the rows it depends on; each wait gives up after
+   `limit` polls (about 128 ns apart; 0 = the default, 2^22), marks the call
+   failed and lets the row go on, so the launch always ends and the next
+   dol_sync() on the stream returns DOL_ERR_TIMEOUT (that call's deltas are
+   then invalid).  stall_sweep 0..7 makes that sweep's rows wait for a flag
+   value no row writes, so every such wait runs out; -1 restores normal
+   operation. */
+DOL_API void       dol_test_wait_hooks(int stall_sweep, unsigned limit);
 
 /* ---- synthetic inputs (no reference counterpart) --------------------------------------
    Integer-exact, so host and device give the same bits.  Value noise: lattice

@@ -9,6 +9,7 @@ bytes (golden_digests.json), which keeps the fixtures a few hundred KB.
 
     python tests/golden/gen_golden.py            # small cases, 1024^2 and 64^3 digests
     python tests/golden/gen_golden.py --full     # adds the benchmarked sizes (a few minutes, ~20 GB RAM)
+    python tests/golden/gen_golden.py --sparse   # adds 1024^3 volumes of 2000 points and of none
 
 --full digests the reference's outputs on the two benchmarked volumes, from
 the same synthetic masks the library generates (its host generator; the
@@ -105,12 +106,16 @@ def main():
     ini = O.init_deltas(m, dims, use_ref=True)
     for meth in ("danielsson", "fastsweep", "jumpflood"):
         dig[f"v64_{meth}_cw1"] = digest(O.propagate(meth, ini, dims, 1, use_ref=True))
+    with open(os.path.join(HERE, "golden_digests.json")) as f:
+        old = json.load(f)
+    kept = ("s3_",) if "--full" in sys.argv else ("c2_", "c3_", "s3_")
+    if "--sparse" in sys.argv:
+        kept = tuple(k for k in kept if k != "s3_")
+    dig.update({k: v for k, v in old.items() if k.startswith(kept)})
     if "--full" in sys.argv:
         dig.update(full_size())
-    else:
-        with open(os.path.join(HERE, "golden_digests.json")) as f:
-            old = json.load(f)
-        dig.update({k: v for k, v in old.items() if k.startswith(("c2_", "c3_"))})
+    if "--sparse" in sys.argv:
+        dig.update(sparse_size())
     with open(os.path.join(HERE, "golden_digests.json"), "w") as f:
         json.dump(dig, f, indent=1, sort_keys=True)
     print("wrote", len(small), "arrays and", len(dig), "digests")
@@ -155,6 +160,23 @@ def full_size():
     bor = O.border_init(m, dims, use_ref=True)
     dig["c3_danielsson_cw2"] = digest(O.propagate("danielsson", bor, dims, 2, use_ref=True))
     print("c3 danielsson", flush=True)
+    return dig
+
+
+def sparse_size():
+    """The reference's signed Felzenszwalb where the other state is far away:
+    1024^3 with 2000 set voxels (BitMaskAddPoints, seed 1) and 1024^3 with none."""
+    threads = os.cpu_count() or 1
+    dig = {}
+    n = 1024
+    dims = (n, n, n)
+    m = O.add_points(np.zeros(O.mask_words(*dims), np.uint32), dims, 2000, 1, use_ref=True)
+    dig["s3_points2000_mask"] = digest(m)
+    dig["s3_points2000_felz_signed"] = digest(_signed_felz_ref(m, dims, threads))
+    print("s3 points", flush=True)
+    m = np.zeros(O.mask_words(*dims), np.uint32)
+    dig["s3_empty_felz_signed"] = digest(_signed_felz_ref(m, dims, threads))
+    print("s3 empty", flush=True)
     return dig
 
 

@@ -370,6 +370,37 @@ def sdf_host(mask_np, dims, method="danielsson", want_deltas=True, want_dist=Tru
 
 # ---- float sites ---------------------------------------------------------------------------------
 
+def init_dirw(mask, dims, out=None, stream=None):
+    """InitDirWFromBitMask: direction-weight planes, float32 (4, h, w) for an
+    image or (8, d, h, w) for a volume, 1 on set cells and 0 elsewhere."""
+    torch = _torch()
+    dims = _dims(dims)
+    planes = 4 if len(dims) == 2 else 8
+    if out is None:
+        out = torch.empty((planes,) + tuple(reversed(dims)), dtype=torch.float32, device=mask.device)
+    fn = lib().dol_init_dirw_2d if len(dims) == 2 else lib().dol_init_dirw_3d
+    check(fn(*_ints(*dims), _ptr(mask), _ptr(out), _stream(stream)))
+    return out
+
+
+def occlusion_sweep(dirw, dims, stream=None):
+    """OcclusionSweep in place: quadrant (2D) or octant (3D) occlusion."""
+    dims = _dims(dims)
+    fn = lib().dol_occlusion_sweep_2d if len(dims) == 2 else lib().dol_occlusion_sweep_3d
+    check(fn(*_ints(*dims), _ptr(dirw), _stream(stream)))
+    return dirw
+
+
+def occlusion_sweep_io(dirw_in, dirw_out, dims, stream=None):
+    """OcclusionSweep(w, h, d, in, out): the octant occlusion caused by `dirw_in`,
+    written to `dirw_out` (each plane's starting cell keeps its value)."""
+    dims = _dims(dims)
+    if len(dims) != 3:
+        raise DolError(ERR_UNSUPPORTED, "the in/out occlusion sweep is 3D, as in the reference")
+    check(lib().dol_occlusion_sweep_3d_io(*_ints(*dims), _ptr(dirw_in), _ptr(dirw_out), _stream(stream)))
+    return dirw_out
+
+
 def gen_sites(n, dims, seed):
     """n float sites uniform in continuous cell coordinates, from the reference's
     LCG (24-bit fractions, drawn x, y[, z] per site); float32 array (n, dim)."""

@@ -575,6 +575,73 @@ dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* deltas, 
     return launched("deltas_to_dist_3d");
 }
 
+// ---- occlusion ----------------------------------------------------------------------------------
+
+constexpr int kMaxOcclusionWidth = 4096;
+
+static dol_status occ_checks(int w, int h, int d)
+{
+    DOL_TRY(check_dims(w, h, d));
+    if (w > kMaxOcclusionWidth)
+        return fail(DOL_ERR_UNSUPPORTED, "occlusion rows are limited to %d cells (got %d)", kMaxOcclusionWidth, w);
+    if ((long long)d * h > (1LL << 40) / 8) return fail(DOL_ERR_INVALID_ARG, "volume too large");
+    return DOL_OK;
+}
+
+dol_status dol_init_dirw_2d(int w, int h, const uint32_t* mask, float* dirW, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, 1));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(dirW, "dirW"));
+    launch_init_dirw(2, mask, dirW, w, h, 1, S(stream));
+    return launched("init_dirw_2d");
+}
+
+dol_status dol_init_dirw_3d(int w, int h, int d, const uint32_t* mask, float* dirW, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    DOL_TRY(check_dev_ptr(dirW, "dirW"));
+    launch_init_dirw(3, mask, dirW, w, h, d, S(stream));
+    return launched("init_dirw_3d");
+}
+
+dol_status dol_occlusion_sweep_2d(int w, int h, float* dirW, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(occ_checks(w, h, 1));
+    DOL_TRY(check_dev_ptr(dirW, "dirW"));
+    launch_occlusion_sweep(2, dirW, nullptr, w, h, 1, S(stream));
+    return launched("occlusion_sweep_2d");
+}
+
+dol_status dol_occlusion_sweep_3d(int w, int h, int d, float* dirW, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(occ_checks(w, h, d));
+    DOL_TRY(check_dev_ptr(dirW, "dirW"));
+    launch_occlusion_sweep(3, dirW, nullptr, w, h, d, S(stream));
+    return launched("occlusion_sweep_3d");
+}
+
+dol_status dol_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(occ_checks(w, h, d));
+    DOL_TRY(check_dev_ptr(in, "in"));
+    DOL_TRY(check_dev_ptr(out, "out"));
+    if (in == out) return fail(DOL_ERR_INVALID_ARG, "the in/out occlusion sweep needs distinct in and out fields");
+    launch_occlusion_sweep(3, out, in, w, h, d, S(stream));
+    return launched("occlusion_sweep_3d_io");
+}
+
 // ---- one-call signed fields ----------------------------------------------------------------------
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }

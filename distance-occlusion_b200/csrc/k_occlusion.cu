@@ -1,0 +1,171 @@
+// k_occlusion.cu -- direction-weight initialisation and the occlusion sweeps.
+//
+// A direction-weight field has 4 (2D) or 8 (3D) planes of w*h[*d] floats;
+// plane `sweep` holds the occlusion seen towards quadrant / octant `sweep`
+// (bit 0: x decreasing, bit 1: y, bit 2: z).  InitDirWFromBitMask
+// (DistanceOcclusionLib.cpp:1114-1146, :2507-2538) writes 1 on set cells and 0
+// elsewhere in every plane.  OcclusionSweep (:1173-1209; 3D :2593-2650, the
+// in/out form :2655-2737) walks a plane from its starting corner -- slices,
+// rows, cells in sweep order -- and updates each cell from its already swept
+// neighbours one step back along x ("left"), y ("up") and z ("back"),
+// neighbours outside the field entering as 0, the corner cell left as it is:
+//     in place:  x += (1 - x) * combine(left, up[, back])
+//     in / out:  out = combine6(out neighbours, in neighbours)
+// with the quadrant / octant combines of :1150-1169 and :2543-2567.
+//
+// Every cell depends on its left neighbour in the same row, so the result is
+// bit-exact only with the reference's serial float chain along x: no
+// reassociation, and every add / multiply rounded on its own (the __f*_rn
+// intrinsics keep the compiler from contracting them into FMAs).  The
+// parallelism is the wavefront: cell (i, j, k) needs (i-1, j, k), (i, j-1, k)
+// and (i, j, k-1).  One CTA sweeps one plane (all planes at once); thread t
+// owns C adjacent columns and walks the (slice, row) items in order, skewed
+// one step behind thread t-1, whose last column it takes from shared memory
+// (double-buffered by step parity); "up" stays in registers and "back" is
+// the thread's own output of h items before.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace dolk {
+
+__device__ __forceinline__ float quad_combine(float a, float b)
+{
+    // 0.75f * ((a + b) - 1.0f * a * b)
+    return __fmul_rn(0.75f, __fsub_rn(__fadd_rn(a, b), __fmul_rn(__fmul_rn(1.0f, a), b)));
+}
+
+__device__ __forceinline__ float oct_combine(float a, float b, float c)
+{
+    // 0.33333333f * (a + b + c - a * b * c)
+    return __fmul_rn(0.33333333f, __fsub_rn(__fadd_rn(__fadd_rn(a, b), c), __fmul_rn(__fmul_rn(a, b), c)));
+}
+
+__device__ __forceinline__ float oct_combine_io(float oa, float ob, float oc, float ia, float ib, float ic)
+{
+    const float a = __fadd_rn(ia, __fmul_rn(__fsub_rn(1.0f, ia), oa));
+    const float b = __fadd_rn(ib, __fmul_rn(__fsub_rn(1.0f, ib), ob));
+    const float c = __fadd_rn(ic, __fmul_rn(__fsub_rn(1.0f, ic), oc));
+    return __fmul_rn(0.3333333f, __fsub_rn(__fadd_rn(__fadd_rn(a, b), c), __fmul_rn(__fmul_rn(a, b), c)));
+}
+
+// x += (1 - x) * q
+__device__ __forceinline__ float occ_update(float x, float q) { return __fadd_rn(x, __fmul_rn(__fsub_rn(1.0f, x), q)); }
+
+// One word of mask (32 cells of a row) per thread; every plane gets the same values.
+__global__ void k_init_dirw(const uint32_t* __restrict__ mask, float* __restrict__ dirw, int w, long long rows,
+                            int planes, long long plane_stride)
+{
+    const int ws = words_per_row(w);
+    const long long words = rows * ws;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / ws;
+        const int k = (int)(i - r * ws);
+        const uint32_t m = mask[i];
+        const int x0 = 32 * k, n = min(32, w - x0);
+        float* row = dirw + r * w + x0;
+        for (int p = 0; p < planes; p++) {
+            float* o = row + p * plane_stride;
+            for (int b = 0; b < n; b++) o[b] = ((m >> b) & 1u) ? 1.0f : 0.0f;
+        }
+    }
+}
+
+template <int DIM, bool IO, int C>
+__global__ void __launch_bounds__(1024) k_occlusion_sweep(float* __restrict__ outp, const float* __restrict__ inp, int w,
+                                                          int h, int d)
+{
+    __shared__ float edge[2][1024];
+    const int sweep = blockIdx.x;
+    const int sx = sweep & 1, sy = (sweep >> 1) & 1, sz = (sweep >> 2) & 1;
+    const int dx = 1 - 2 * sx, dy = 1 - 2 * sy, dz = 1 - 2 * sz;
+    const long long wh = (long long)w * h;
+    const long long n = wh * d;
+    float* out = outp + sweep * n;
+    const float* in = IO ? inp + sweep * n : nullptr;
+    const int t = threadIdx.x;
+    const int T = (w + C - 1) / C;   // threads holding columns (the rest only keep the barriers)
+    const int ii0 = t * C;
+    const int ncol = max(0, min(C, w - ii0));
+    float up[C];
+#pragma unroll
+    for (int u = 0; u < C; u++) up[u] = 0.0f;
+    const long long Q = (long long)d * h;
+    for (long long s = 0; s < Q + T - 1; s++) {
+        const long long q = s - t;
+        float last = 0.0f;
+        if (q >= 0 && q < Q && ncol > 0) {
+            const int kk = (int)(q / h), jj = (int)(q - (long long)kk * h);
+            const int y = sy ? h - 1 - jj : jj, z = sz ? d - 1 - kk : kk;
+            const long long rowbase = ((long long)z * h + y) * w;
+            float left = ii0 > 0 ? edge[(s - 1) & 1][t - 1] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < C; u++) {
+                if (u < ncol) {
+                    const int ii = ii0 + u;
+                    const long long c = rowbase + (sx ? w - 1 - ii : ii);
+                    const float upv = jj ? up[u] : 0.0f;
+                    const float back = DIM == 3 && kk ? out[c - dz * wh] : 0.0f;
+                    float v;
+                    if (ii == 0 && jj == 0 && kk == 0) {
+                        v = out[c];   // the starting corner keeps its value
+                    } else if (IO) {
+                        const float il = ii ? in[c - dx] : 0.0f;
+                        const float iu = jj ? in[c - (long long)dy * w] : 0.0f;
+                        const float ib = kk ? in[c - dz * wh] : 0.0f;
+                        v = oct_combine_io(left, upv, back, il, iu, ib);
+                        out[c] = v;
+                    } else {
+                        const float qv = DIM == 2 ? quad_combine(left, upv) : oct_combine(left, upv, back);
+                        v = occ_update(out[c], qv);
+                        out[c] = v;
+                    }
+                    up[u] = v;
+                    left = v;
+                }
+            }
+            last = left;
+        }
+        edge[s & 1][t] = last;
+        __syncthreads();
+    }
+}
+
+void launch_init_dirw(int dim, const uint32_t* mask, float* dirw, int w, int h, int d, cudaStream_t st)
+{
+    const long long rows = (long long)h * (dim == 3 ? d : 1);
+    const long long words = rows * words_per_row(w);
+    long long blocks = (words + 255) / 256;
+    const long long cap = (long long)g_num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    ProfScope ps("init_dirw", st);
+    k_init_dirw<<<(int)blocks, 256, 0, st>>>(mask, dirw, w, rows, dim == 3 ? 8 : 4, (long long)w * rows);
+}
+
+void launch_occlusion_sweep(int dim, float* dirw, const float* in, int w, int h, int d, cudaStream_t st)
+{
+    const int C = w <= 1024 ? 1 : (w <= 2048 ? 2 : 4);
+    int T = (w + C - 1) / C;
+    T = (T + 31) & ~31;
+    const int planes = dim == 3 ? 8 : 4;
+    const int dd = dim == 3 ? d : 1;
+    ProfScope ps(in ? "occlusion_sweep_io" : "occlusion_sweep", st);
+#define DOL_OCC_CASE(DIMV, IOV, CV) \
+    k_occlusion_sweep<DIMV, IOV, CV><<<planes, T, 0, st>>>(dirw, in, w, h, dd)
+    if (dim == 2) {
+        if (C == 1) DOL_OCC_CASE(2, false, 1);
+        else if (C == 2) DOL_OCC_CASE(2, false, 2);
+        else DOL_OCC_CASE(2, false, 4);
+    } else if (!in) {
+        if (C == 1) DOL_OCC_CASE(3, false, 1);
+        else if (C == 2) DOL_OCC_CASE(3, false, 2);
+        else DOL_OCC_CASE(3, false, 4);
+    } else {
+        if (C == 1) DOL_OCC_CASE(3, true, 1);
+        else if (C == 2) DOL_OCC_CASE(3, true, 2);
+        else DOL_OCC_CASE(3, true, 4);
+    }
+#undef DOL_OCC_CASE
+}
+
+}  // namespace dolk

@@ -124,6 +124,11 @@ void launch_chamfer_2d(T* dist, int w, int h, cudaStream_t st);
 template <typename T>
 void launch_init_distances_int(const uint32_t* mask, T* dist, int w, long long rows, T max_d, cudaStream_t st);
 
+// k_occlusion.cu -- direction-weight planes (4 in 2D, 8 in 3D) and the
+// occlusion sweeps; in != nullptr selects the 3D in/out form (rows up to 4096)
+void launch_init_dirw(int dim, const uint32_t* mask, float* dirw, int w, int h, int d, cudaStream_t st);
+void launch_occlusion_sweep(int dim, float* dirw, const float* in, int w, int h, int d, cudaStream_t st);
+
 // k_sites.cu
 void launch_sites_seed(int dim, int w, int h, int d, int n, const float* sites, uint32_t* mask, int* cell_site,
                        cudaStream_t st);

@@ -128,6 +128,49 @@ namespace DOL
         InPlace(distances, (size_t)w * h, [&](float* d) { Check(dol_felzenszwalb_2d(w, h, d, nullptr, 0, nullptr)); });
     }
 
+    // --- occlusion -----------------------------------------------------------------
+    void InitDirWFromBitMask(int w, int h, const uint32_t mask[], float dirW4[])
+    {
+        const size_t n = 4 * (size_t)w * h * sizeof(float);
+        Dev dm(MaskBytes(w, h, 1)), dd(n);
+        dm.up(mask, MaskBytes(w, h, 1));
+        Check(dol_init_dirw_2d(w, h, dm.as<uint32_t>(), dd.as<float>(), nullptr));
+        Finish();
+        dd.down(dirW4, n);
+    }
+
+    void InitDirWFromBitMask(int w, int h, int d, const uint32_t mask[], float dirW8[])
+    {
+        const size_t n = 8 * (size_t)w * h * d * sizeof(float);
+        Dev dm(MaskBytes(w, h, d)), dd(n);
+        dm.up(mask, MaskBytes(w, h, d));
+        Check(dol_init_dirw_3d(w, h, d, dm.as<uint32_t>(), dd.as<float>(), nullptr));
+        Finish();
+        dd.down(dirW8, n);
+    }
+
+    void OcclusionSweep(int w, int h, float dirW4[])
+    {
+        InPlace(dirW4, 4 * (size_t)w * h, [&](float* p) { Check(dol_occlusion_sweep_2d(w, h, p, nullptr)); });
+    }
+
+    void OcclusionSweep(int w, int h, int d, float dirW8[])
+    {
+        InPlace(dirW8, 8 * (size_t)w * h * d, [&](float* p) { Check(dol_occlusion_sweep_3d(w, h, d, p, nullptr)); });
+    }
+
+    void OcclusionSweep(int w, int h, int d, const float inDirW8[], float outDirW8[])
+    {
+        // out goes up too: the reference leaves each plane's starting cell as it was
+        const size_t n = 8 * (size_t)w * h * d * sizeof(float);
+        Dev di(n), dout(n);
+        di.up(inDirW8, n);
+        dout.up(outDirW8, n);
+        Check(dol_occlusion_sweep_3d_io(w, h, d, di.as<float>(), dout.as<float>(), nullptr));
+        Finish();
+        dout.down(outDirW8, n);
+    }
+
     void InitDeltasFromBitMask(int w, int h, const uint32_t mask[], cCellDelta2 delta[], bool invert)
     {
         Dev dm(MaskBytes(w, h, 1)), dd((size_t)w * h * sizeof(cCellDelta2));

@@ -10,9 +10,9 @@
 // directly and skip the copies.  Failures throw DOL::Error (the reference has
 // no error reporting; it would crash or write out of bounds instead).
 //
-// The occlusion routines of the reference (InitDirWFromBitMask,
-// OcclusionSweep, ShadowSweep, Encode*) are not provided here: they stay with
-// the reference library on the host.
+// Of the reference's occlusion routines, InitDirWFromBitMask and
+// OcclusionSweep run here on the GPU; ShadowSweep, InitOccFromBitMask and the
+// Encode* helpers stay with the reference library on the host.
 #ifndef DISTANCE_OCCLUSION_B200_H
 #define DISTANCE_OCCLUSION_B200_H
 
@@ -72,6 +72,13 @@ namespace DOL
     void Danielsson(int w, int h, int d, cCellDelta3 delta[], int cw = 1);
     void JumpFlood (int w, int h,        cCellDelta2 delta[], int cw = 1);
     void JumpFlood (int w, int h, int d, cCellDelta3 delta[], int cw = 1);
+
+    // --- occlusion: direction-weight planes (4 in 2D, 8 in 3D) and their sweeps --------
+    void InitDirWFromBitMask(int w, int h,        const uint32_t mask[], float dirW4[]);
+    void InitDirWFromBitMask(int w, int h, int d, const uint32_t mask[], float dirW8[]);
+    void OcclusionSweep(int w, int h,        float dirW4[]);
+    void OcclusionSweep(int w, int h, int d, float dirW8[]);
+    void OcclusionSweep(int w, int h, int d, const float inDirW8[], float outDirW8[]);
 
     // --- additions with no reference counterpart -----------------------------------
     // Exact EDT straight from the mask: form 0 squared, 1 distance, 2 signed

@@ -182,6 +182,21 @@ DOL_API dol_status dol_deltas_to_dist_2d(int w, int h, const dol_delta2* deltas,
 DOL_API dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* deltas, int cw,
                                  const uint32_t* sign_mask, float* out, void* stream);
 
+/* ---- occlusion -------------------------------------------------------------------------
+   Direction-weight fields: 4 (2D) or 8 (3D) planes of w*h[*d] floats, plane s
+   for quadrant / octant s (bit 0: x decreasing, bit 1: y, bit 2: z).
+   InitDirWFromBitMask (DistanceOcclusionLib.cpp:1114-1146, :2507-2538): 1 on set
+   cells, 0 elsewhere, in every plane.
+   OcclusionSweep (DistanceOcclusionLib.cpp:1173-1209, :2745-2769), in place;
+   the 3D in/out form (:2771-2784) writes the occlusion caused by `in` to `out`
+   (out's starting-corner cell of each plane is left as it was).  Bit-exact:
+   the reference's float operations in its order.  Rows up to 4096 cells. */
+DOL_API dol_status dol_init_dirw_2d(int w, int h, const uint32_t* mask, float* dirW, void* stream);
+DOL_API dol_status dol_init_dirw_3d(int w, int h, int d, const uint32_t* mask, float* dirW, void* stream);
+DOL_API dol_status dol_occlusion_sweep_2d(int w, int h, float* dirW, void* stream);
+DOL_API dol_status dol_occlusion_sweep_3d(int w, int h, int d, float* dirW, void* stream);
+DOL_API dol_status dol_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out, void* stream);
+
 /* ---- one-call fields (the tool's Generate* paths) ----------------------------------- */
 /* Signed border-initialised distance field (GenerateSignedDistanceBorder,
    DistanceOcclusionTool.cpp:1333-1365 / :1471-1498): border init, `method`

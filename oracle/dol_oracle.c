@@ -13,6 +13,7 @@
 
 #include <float.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -936,4 +937,85 @@ void dolo_edt_brute(int w, int h, int d, const uint32_t* mask, float* out)
                 out[((size_t)z * h + y) * w + x] = best < 0 ? FLT_MAX : (float)best;
             }
     free(pts);
+}
+
+/* ---- occlusion sweeps -------------------------------------------------------
+ * Direction-weight fields: 4 (2D) or 8 (3D) planes of w*h[*d] floats, plane
+ * `sweep` holding the occlusion seen towards quadrant / octant `sweep`
+ * (bit 0: x decreasing, bit 1: y, bit 2: z).  InitDirWFromBitMask
+ * (DistanceOcclusionLib.cpp:1114-1146, :2507-2538) sets every plane to 1 on
+ * set cells and 0 elsewhere.  A sweep (:1173-1209, :2593-2650, in/out form
+ * :2655-2737) walks its plane from the corner it starts at: slices in z order,
+ * rows in y order, cells in x order, each cell combining the already swept
+ * neighbours one step back along x ("left"), y ("up") and z ("back"); a
+ * neighbour outside the field enters as 0, and the corner cell itself is left
+ * as it is.  Quadrant combine (:1150-1169) and octant combines (:2543-2567)
+ * are evaluated in the reference's float operations and order; this file is
+ * built without contraction so no step fuses. */
+
+static inline float quad_combine(float a, float b) { return 0.75f * ((a + b) - 1.0f * a * b); }
+static inline float oct_combine(float a, float b, float c) { return 0.33333333f * (a + b + c - a * b * c); }
+static inline float oct_combine_io(float oa, float ob, float oc, float ia, float ib, float ic)
+{
+    float a = ia + (1.0f - ia) * oa;
+    float b = ib + (1.0f - ib) * ob;
+    float c = ic + (1.0f - ic) * oc;
+    return 0.3333333f * (a + b + c - a * b * c);
+}
+
+void dolo_init_dirw(int w, int h, int d, int planes, const uint32_t* mask, float* dirW)
+{
+    size_t n = (size_t)w * h * d;
+    int ws = words_per_row(w);
+    for (size_t r = 0; r < (size_t)h * d; r++)
+        for (int x = 0; x < w; x++) {
+            float v = mask_bit(mask + r * ws, x) ? 1.0f : 0.0f;
+            for (int p = 0; p < planes; p++) dirW[(size_t)p * n + r * w + x] = v;
+        }
+}
+
+/* one plane: in == NULL updates it in place (x += (1 - x) * combine), else
+ * writes combine of (out, in) neighbours to out (3D only) */
+static void occ_plane(int w, int h, int d, int sweep, int dim, const float* in, float* out)
+{
+    int sx = sweep & 1, sy = (sweep >> 1) & 1, sz = (sweep >> 2) & 1;
+    int dx = 1 - 2 * sx, dy = 1 - 2 * sy, dz = 1 - 2 * sz;
+    size_t wh = (size_t)w * h;
+    for (int kk = 0; kk < d; kk++) {
+        int z = sz ? d - 1 - kk : kk;
+        for (int jj = 0; jj < h; jj++) {
+            int y = sy ? h - 1 - jj : jj;
+            for (int ii = 0; ii < w; ii++) {
+                int x = sx ? w - 1 - ii : ii;
+                if (ii == 0 && jj == 0 && kk == 0) continue;   /* the starting corner */
+                size_t c = (size_t)z * wh + (size_t)y * w + x;
+                size_t cl = c - dx, cu = c - (ptrdiff_t)dy * w, cb = c - (ptrdiff_t)dz * (ptrdiff_t)wh;
+                float ol = ii ? out[cl] : 0.0f, ou = jj ? out[cu] : 0.0f, ob = kk ? out[cb] : 0.0f;
+                if (in) {
+                    float il = ii ? in[cl] : 0.0f, iu = jj ? in[cu] : 0.0f, ib = kk ? in[cb] : 0.0f;
+                    out[c] = oct_combine_io(ol, ou, ob, il, iu, ib);
+                } else {
+                    float q = dim == 2 ? quad_combine(ol, ou) : oct_combine(ol, ou, ob);
+                    out[c] += (1.0f - out[c]) * q;
+                }
+            }
+        }
+    }
+}
+
+void dolo_occlusion_sweep_2d(int w, int h, float* dirW)
+{
+    for (int s = 0; s < 4; s++) occ_plane(w, h, 1, s, 2, NULL, dirW + (size_t)s * w * h);
+}
+
+void dolo_occlusion_sweep_3d(int w, int h, int d, float* dirW)
+{
+    size_t n = (size_t)w * h * d;
+    for (int s = 0; s < 8; s++) occ_plane(w, h, d, s, 3, NULL, dirW + (size_t)s * n);
+}
+
+void dolo_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out)
+{
+    size_t n = (size_t)w * h * d;
+    for (int s = 0; s < 8; s++) occ_plane(w, h, d, s, 3, in + (size_t)s * n, out + (size_t)s * n);
 }

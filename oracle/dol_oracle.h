@@ -86,6 +86,13 @@ void dolo_deltas_to_dist_3d(int w, int h, int d, const int16_t* deltas, int cw, 
    cells with no set cell anywhere get FLT_MAX */
 void dolo_edt_brute(int w, int h, int d, const uint32_t* mask, float* out);
 
+/* occlusion: direction-weight planes (4 for 2D, 8 for 3D) from a mask, and the
+   quadrant / octant sweeps in place (2D, 3D) or from in to out (3D) */
+void dolo_init_dirw(int w, int h, int d, int planes, const uint32_t* mask, float* dirW);
+void dolo_occlusion_sweep_2d(int w, int h, float* dirW);
+void dolo_occlusion_sweep_3d(int w, int h, int d, float* dirW);
+void dolo_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -322,3 +322,40 @@ def edt_brute(mask, dims):
     out = np.empty(d3[0] * d3[1] * d3[2], dtype=np.float32)
     lib().dolo_edt_brute(*_i(*d3), _p(mask), _p(out))
     return out.reshape(tuple(reversed(dims)))
+
+
+# ---- occlusion ---------------------------------------------------------------------------
+
+def init_dirw(mask, dims, use_ref=False):
+    """InitDirWFromBitMask: float32[planes, (d,) h, w], planes = 4 (2D) / 8 (3D)."""
+    planes = 4 if len(dims) == 2 else 8
+    out = np.empty((planes,) + tuple(reversed(dims)), dtype=np.float32)
+    if use_ref:
+        if len(dims) == 2:
+            ref().ref_init_dirw_2d(*_i(*dims), _p(mask), _p(out))
+        else:
+            ref().ref_init_dirw_3d(*_i(*dims), _p(mask), _p(out))
+    else:
+        d3 = list(dims) + [1] * (3 - len(dims))
+        lib().dolo_init_dirw(*_i(*d3), C.c_int(planes), _p(mask), _p(out))
+    return out
+
+
+def occlusion_sweep(dirw, dims, use_ref=False):
+    """OcclusionSweep in place (2D quadrants / 3D octants), on a copy."""
+    out = np.ascontiguousarray(dirw, dtype=np.float32).copy()
+    pre, L = ("ref_", ref()) if use_ref else ("dolo_", lib())
+    if len(dims) == 2:
+        getattr(L, pre + "occlusion_sweep_2d")(*_i(*dims), _p(out))
+    else:
+        getattr(L, pre + "occlusion_sweep_3d")(*_i(*dims), _p(out))
+    return out
+
+
+def occlusion_sweep_io(dirw_in, dirw_out, dims, use_ref=False):
+    """OcclusionSweep(w, h, d, in, out): octant occlusion of `in` written to a copy of `out`."""
+    src = np.ascontiguousarray(dirw_in, dtype=np.float32)
+    out = np.ascontiguousarray(dirw_out, dtype=np.float32).copy()
+    pre, L = ("ref_", ref()) if use_ref else ("dolo_", lib())
+    getattr(L, pre + "occlusion_sweep_3d_io")(*_i(*dims), _p(src), _p(out))
+    return out

@@ -44,6 +44,11 @@ void ref_init_distances_2d_i16(int w, int h, const uint32_t* mask, int16_t* dist
 void ref_init_distances_2d_i32(int w, int h, const uint32_t* mask, int32_t* dist, int32_t max_d) { DOL::InitDistancesFromBitMask(w, h, mask, dist, max_d); }
 int ref_chamfer_2d_i16(int w, int h, int16_t* dist) { return DOL::Chamfer(w, h, dist); }
 int ref_chamfer_2d_i32(int w, int h, int32_t* dist) { return DOL::Chamfer(w, h, dist); }
+void ref_init_dirw_2d(int w, int h, const uint32_t* mask, float* dirW) { DOL::InitDirWFromBitMask(w, h, mask, dirW); }
+void ref_init_dirw_3d(int w, int h, int d, const uint32_t* mask, float* dirW) { DOL::InitDirWFromBitMask(w, h, d, mask, dirW); }
+void ref_occlusion_sweep_2d(int w, int h, float* dirW) { DOL::OcclusionSweep(w, h, dirW); }
+void ref_occlusion_sweep_3d(int w, int h, int d, float* dirW) { DOL::OcclusionSweep(w, h, d, dirW); }
+void ref_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out) { DOL::OcclusionSweep(w, h, d, in, out); }
 
 /* 3D restatement on the reference's own 1D routine: z, then y, then x.  Lines
  * are split over `threads` host threads, each with private v/z/line scratch

@@ -7,8 +7,8 @@
  * library is one file; every function the B200 C++ interface
  * (distance-occlusion_b200/shim/DistanceOcclusionB200.h) provides is renamed
  * here by the preprocessor before the file is included as it lies, so this
- * translation unit defines only the rest -- BruteForce, the occlusion and
- * shadow sweeps, the Encode* helpers -- under their own names, and its copies
+ * translation unit defines only the rest -- BruteForce, the shadow sweep,
+ * InitOccFromBitMask, the Encode* helpers -- under their own names, and its copies
  * of the distance functions under names nothing calls.  The tool's calls of
  * DOL::Danielsson, DOL::InitBorderDeltasFromBitMask, ... then resolve to the
  * GPU library at link time; `nm` on the linked tool shows them undefined.
@@ -26,5 +26,7 @@
 #define FastSweep                   FastSweep_RefHost
 #define Danielsson                  Danielsson_RefHost
 #define JumpFlood                   JumpFlood_RefHost
+#define InitDirWFromBitMask         InitDirWFromBitMask_RefHost
+#define OcclusionSweep              OcclusionSweep_RefHost
 
 #include "DistanceOcclusionLib.cpp"

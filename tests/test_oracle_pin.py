@@ -272,3 +272,25 @@ def test_readme_sdf_images_within_one_level(O, name):
     enc, want = _readme_case(O, name)
     diff = np.abs(enc - want)
     assert diff.max() <= 1, f"max grey-level difference {diff.max()}"
+
+
+# ---- occlusion sweeps ----------------------------------------------------------------------
+
+@pytest.mark.parametrize("dims", [(1, 1), (1, 7), (7, 1), (31, 9), (33, 20), (64, 64), (100, 37),
+                                  (1, 1, 1), (5, 1, 3), (9, 7, 5), (33, 6, 5), (24, 20, 16)])
+def test_occlusion_matches_reference(O, dims):
+    if O.ref() is None:
+        pytest.skip("reference build (oracle/_ref) absent")
+    rng = np.random.default_rng(sum(dims) + 41)
+    for p in (0.0, 0.05, 0.3, 0.8, 1.0):
+        m = O.bool_to_mask(rng.random(tuple(reversed(dims))) < p)
+        dw = O.init_dirw(m, dims)
+        np.testing.assert_array_equal(dw, O.init_dirw(m, dims, use_ref=True))
+        got = O.occlusion_sweep(dw, dims)
+        want = O.occlusion_sweep(dw, dims, use_ref=True)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=f"{dims} p={p}")
+        if len(dims) == 3:
+            prior = rng.random(dw.shape).astype(np.float32)   # cells the reference leaves unwritten keep this
+            got = O.occlusion_sweep_io(dw, prior, dims)
+            want = O.occlusion_sweep_io(dw, prior, dims, use_ref=True)
+            np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=f"io {dims} p={p}")

@@ -7,8 +7,9 @@ twice from the same sources: distocc_ref with the reference library, as the
 reference's Makefile does, and distocc_b200 with tool_ref_half.cpp (the
 reference library minus every function the B200 library provides) and
 libdol_b200.so.  The CPU test checks the link: in distocc_b200 the distance
-functions are undefined, to be bound to libdol_b200.so at load time, while
-the occlusion routines and BruteForce stay defined from the reference.  The
+functions and the occlusion sweeps are undefined, to be bound to
+libdol_b200.so at load time, while BruteForce and the shadow sweep stay
+defined from the reference.  The
 GPU test runs both tools on the same command lines and compares every image
 they write, byte for byte.
 """
@@ -25,8 +26,9 @@ TOOL_REF = os.path.join(REF, "distocc_ref")
 TOOL_B200 = os.path.join(REF, "distocc_b200")
 
 GPU_SIDE = ["InitDistancesFromBitMask", "Chamfer", "Felzenszwalb", "InitDeltasFromBitMask",
-            "InitBorderDeltasFromBitMask", "FastSweep", "Danielsson", "JumpFlood"]
-REF_SIDE = ["BruteForce", "InitDirWFromBitMask", "OcclusionSweep", "ShadowSweep"]
+            "InitBorderDeltasFromBitMask", "FastSweep", "Danielsson", "JumpFlood", "InitDirWFromBitMask",
+            "OcclusionSweep"]
+REF_SIDE = ["BruteForce", "ShadowSweep"]
 
 
 def _need_tools():
@@ -81,6 +83,10 @@ COMMANDS = [
     "-S -W 40 -p 20 -m 0",
     "-s -W 24 20 16 -p 10 -c",
     "-x -w 128 -p 20",
+    "-x -w 300 200 -b 4 -p 30 5 -m 2",
+    "-x -W 32 -p 20",
+    "-x -W 40 30 20 -b 6 -p 30 -m 1",
+    "-x -W 24 -p 10 -m 2",
 ]
 
 

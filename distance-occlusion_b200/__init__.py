@@ -70,7 +70,8 @@ def lib():
                      "dol_fastsweep_3d_workspace_size", "dol_felzenszwalb_2d_workspace_size",
                      "dol_edt_mask_2d_workspace_size", "dol_edt_mask_3d_workspace_size", "dol_sdf_workspace_size",
                      "dol_sdf_two_pass_workspace_size",
-                     "dol_batch_workspace_size", "dol_sites_backward_workspace_size"):
+                     "dol_batch_workspace_size", "dol_sites_backward_workspace_size",
+                     "dol_danielsson_workspace_size"):
             getattr(L, name).restype = C.c_size_t
         _lib = L
     return _lib

@@ -104,6 +104,12 @@ dol_status launched(const char* what)
     return DOL_OK;
 }
 
+// Largest workspace the library allocates by itself (0: no limit); above it
+// an entry point reports DOL_ERR_NO_MEMORY, Danielsson runs its serial engine.
+std::atomic<size_t> g_workspace_limit{0};
+// which Danielsson engine this thread's last call queued (dol_last_engine)
+thread_local int t_engine = 0;
+
 // Workspace: the caller's, or a stream-ordered allocation freed after the work.
 struct Workspace {
     void* ptr = nullptr;
@@ -127,6 +133,10 @@ dol_status get_workspace(Workspace& ws, void* user, size_t user_bytes, size_t ne
         ws.ptr = user;
         return DOL_OK;
     }
+    const size_t cap = g_workspace_limit.load(std::memory_order_relaxed);
+    if (cap && need > cap)
+        return fail(DOL_ERR_NO_MEMORY, "workspace of %zu bytes exceeds the limit of %zu set by dol_set_workspace_limit",
+                    need, cap);
     cudaError_t e = cudaMallocAsync(&ws.ptr, need, st);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -404,22 +414,13 @@ dol_status dol_init_border_3d(int w, int h, int d, const uint32_t* mask, dol_del
 
 // ---- propagation -------------------------------------------------------------------------
 
-dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* stream)
-{
-    DeviceState* ds;
-    DOL_TRY(device_state(&ds));
-    DOL_TRY(check_dims(w, h, 1));
-    DOL_TRY(check_cw(cw));
-    DOL_TRY(check_sweep_width(w));
-    DOL_TRY(check_dev_ptr(deltas, "deltas"));
-    Workspace ws;
-    const size_t need = danielsson_workspace_bytes(2, w, h, 1);
-    if (get_workspace(ws, nullptr, 0, need, S(stream)) != DOL_OK) ws.ptr = nullptr;   // serial engine needs none
-    run_danielsson(2, deltas, w, h, 1, cw, ws.ptr, need, ds->err_dev, S(stream));
-    return launched("danielsson_2d");
-}
-
-dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* stream)
+// The Danielsson entries: the block schedule on the caller's workspace or
+// one the library allocates; without one (the allocation failed, or it is
+// above the dol_set_workspace_limit cap), the serial engine, which needs no
+// workspace but is much slower on large fields -- dol_last_engine() and
+// dol_last_error() say so.
+static dol_status danielsson_common(int dim, int w, int h, int d, void* deltas, int cw, void* workspace,
+                                    size_t workspace_bytes, bool caller_ws, void* stream)
 {
     DeviceState* ds;
     DOL_TRY(device_state(&ds));
@@ -427,12 +428,58 @@ dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, vo
     DOL_TRY(check_cw(cw));
     DOL_TRY(check_sweep_width(w));
     DOL_TRY(check_dev_ptr(deltas, "deltas"));
+    const int dd = dim == 3 ? d : 1;
+    const size_t need = danielsson_workspace_bytes(dim, w, h, dd);
     Workspace ws;
-    const size_t need = danielsson_workspace_bytes(3, w, h, d);
-    if (get_workspace(ws, nullptr, 0, need, S(stream)) != DOL_OK) ws.ptr = nullptr;   // serial engine needs none
-    run_danielsson(3, deltas, w, h, d, cw, ws.ptr, need, ds->err_dev, S(stream));
-    return launched("danielsson_3d");
+    std::string why;
+    if (caller_ws && workspace) {
+        DOL_TRY(get_workspace(ws, workspace, workspace_bytes, need, S(stream)));
+    } else if (need && get_workspace(ws, nullptr, 0, need, S(stream)) != DOL_OK) {
+        why = t_err;   // the failed allocation's message
+        ws.ptr = nullptr;
+    }
+    const bool blocks = run_danielsson(dim, deltas, w, h, dd, cw, ws.ptr, need, ds->err_dev, S(stream));
+    t_engine = blocks ? DOL_ENGINE_BLOCKS : DOL_ENGINE_SERIAL;
+    dol_status st = launched(dim == 3 ? "danielsson_3d" : "danielsson_2d");
+    if (st == DOL_OK)
+        t_err = blocks ? std::string()
+                       : (need ? "danielsson: serial engine (no workspace for the block schedule: " +
+                                     (why.empty() ? std::string("none given") : why) + ")"
+                               : "danielsson: serial engine (the block schedule does not apply to this shape)");
+    return st;
 }
+
+size_t dol_danielsson_workspace_size(int w, int h, int d)
+{
+    if (w < 1 || h < 1 || d < 1) return 0;
+    return danielsson_workspace_bytes(d > 1 ? 3 : 2, w, h, d);
+}
+
+dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* stream)
+{
+    return danielsson_common(2, w, h, 1, deltas, cw, nullptr, 0, false, stream);
+}
+
+dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* stream)
+{
+    return danielsson_common(3, w, h, d, deltas, cw, nullptr, 0, false, stream);
+}
+
+dol_status dol_danielsson_2d_ws(int w, int h, dol_delta2* deltas, int cw, void* workspace, size_t workspace_bytes,
+                                void* stream)
+{
+    return danielsson_common(2, w, h, 1, deltas, cw, workspace, workspace_bytes, true, stream);
+}
+
+dol_status dol_danielsson_3d_ws(int w, int h, int d, dol_delta3* deltas, int cw, void* workspace,
+                                size_t workspace_bytes, void* stream)
+{
+    return danielsson_common(3, w, h, d, deltas, cw, workspace, workspace_bytes, true, stream);
+}
+
+int dol_last_engine(void) { return t_engine; }
+
+void dol_set_workspace_limit(size_t bytes) { g_workspace_limit.store(bytes, std::memory_order_relaxed); }
 
 dol_status dol_fastsweep_2d(int w, int h, dol_delta2* deltas, int cw, void* stream)
 {

@@ -532,14 +532,15 @@ size_t danielsson_workspace_bytes(int dim, int w, int h, int d)
     return dan_blocks_workspace_bytes(dim, w, h, d, R);
 }
 
-void run_danielsson(int dim, void* deltas, int w, int h, int d, int cw, void* ws, size_t ws_bytes, int* err,
+bool run_danielsson(int dim, void* deltas, int w, int h, int d, int cw, void* ws, size_t ws_bytes, int* err,
                     cudaStream_t st)
 {
     const int R = dan_blocks_rows(dim, w, h, d);
     if (ws && R < kDanSerial && ws_bytes >= dan_blocks_workspace_bytes(dim, w, h, d, R) &&
         launch_danielsson_blocks(dim, deltas, w, h, d, cw, R, ws, err, st))
-        return;
+        return true;
     launch_danielsson(dim, deltas, w, h, d, cw, st);
+    return false;
 }
 
 bool launch_danielsson_blocks(int dim, void* deltas, int w, int h, int d, int cw, int R, void* ws, int* err,

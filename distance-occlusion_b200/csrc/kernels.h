@@ -109,7 +109,8 @@ bool launch_danielsson_blocks(int dim, void* deltas, int w, int h, int d, int cw
 // the Danielsson entry used by the C ABI: the block schedule when its
 // workspace is given and the shape calls for it, else the serial engine
 size_t danielsson_workspace_bytes(int dim, int w, int h, int d);
-void run_danielsson(int dim, void* deltas, int w, int h, int d, int cw, void* ws, size_t ws_bytes, int* err,
+// true when the block schedule ran, false for the serial engine
+bool run_danielsson(int dim, void* deltas, int w, int h, int d, int cw, void* ws, size_t ws_bytes, int* err,
                     cudaStream_t st);
 void launch_fastsweep_2d(void* deltas, int w, int h, int cw, cudaStream_t st);
 size_t fastsweep3_workspace_bytes(int w, int h, int d);

@@ -82,6 +82,11 @@ DOL_API int         dol_version(void);
 DOL_API const char* dol_status_string(dol_status s);
 DOL_API const char* dol_last_error(void);            /* detail of the last failure on this thread */
 DOL_API dol_status  dol_sync(void* stream);          /* wait for the stream, report device errors */
+/* Caps the scratch the library allocates by itself (0: no cap, the default);
+   process-wide.  Entry points needing more return DOL_ERR_NO_MEMORY, except
+   Danielsson, which then runs its serial engine (see dol_last_engine).
+   No reference counterpart. */
+DOL_API void        dol_set_workspace_limit(size_t bytes);
 
 /* ---- bitmasks --------------------------------------------------------------- */
 /* MaskSize (DistanceOcclusionLib.h:124-135); d = 1 for images */
@@ -115,9 +120,25 @@ DOL_API dol_status dol_init_border_2d(int w, int h, const uint32_t* mask, dol_de
 DOL_API dol_status dol_init_border_3d(int w, int h, int d, const uint32_t* mask, dol_delta3* deltas, void* stream);
 
 /* ---- delta propagation (in place) ------------------------------------------------- */
-/* Danielsson (DistanceOcclusionLib.cpp:702-778, :2348-2394) */
+/* Danielsson (DistanceOcclusionLib.cpp:702-778, :2348-2394).  Large fields
+   run as an exact block schedule that needs scratch of
+   dol_danielsson_workspace_size() bytes (about 2.2x the field for volumes);
+   the plain entries allocate it stream-ordered, the _ws entries take the
+   caller's (NULL: allocate; too small: DOL_ERR_INVALID_ARG).  Without it --
+   the allocation failed or is above the dol_set_workspace_limit cap -- the
+   serial engine runs instead: same deltas, far slower on large fields; the
+   call still returns DOL_OK, and dol_last_engine() / dol_last_error() say so. */
 DOL_API dol_status dol_danielsson_2d(int w, int h, dol_delta2* deltas, int cw, void* stream);
 DOL_API dol_status dol_danielsson_3d(int w, int h, int d, dol_delta3* deltas, int cw, void* stream);
+DOL_API size_t     dol_danielsson_workspace_size(int w, int h, int d);   /* d = 1 for images; 0: none used */
+DOL_API dol_status dol_danielsson_2d_ws(int w, int h, dol_delta2* deltas, int cw, void* workspace,
+                                        size_t workspace_bytes, void* stream);
+DOL_API dol_status dol_danielsson_3d_ws(int w, int h, int d, dol_delta3* deltas, int cw, void* workspace,
+                                        size_t workspace_bytes, void* stream);
+/* the engine this thread's last Danielsson call queued (no reference counterpart) */
+#define DOL_ENGINE_BLOCKS 1   /* exact block schedule on a workspace */
+#define DOL_ENGINE_SERIAL 2   /* serial single-CTA engine, no workspace */
+DOL_API int        dol_last_engine(void);
 /* FastSweep (DistanceOcclusionLib.cpp:633-697, :2186-2260) */
 DOL_API dol_status dol_fastsweep_2d(int w, int h, dol_delta2* deltas, int cw, void* stream);
 DOL_API size_t     dol_fastsweep_3d_workspace_size(int w, int h, int d);

@@ -113,3 +113,56 @@ def test_blocks_match_serial_engine(dol, O, cuda, tune):
     assert cuda.equal(a, b)
     want = O.propagate("danielsson", O.border_init(md.cpu().numpy().view(np.uint32), dims), dims, 2)
     np.testing.assert_array_equal(a.cpu().numpy(), want)
+
+
+# ---- workspace: the caller's, the library's, or none (serial engine, reported) ----------------
+
+ENGINE_BLOCKS, ENGINE_SERIAL = 1, 2
+
+
+@pytest.mark.parametrize("dims", [(300, 257), (96, 80, 40)])
+def test_danielsson_workspace_paths_agree_and_fallback_is_reported(dol, O, cuda, dims):
+    """The block schedule on the caller's workspace (the _ws entries), on the
+    library's own allocation, and -- with the library's allocations capped
+    below the workspace size -- the serial engine: identical deltas, equal to
+    the oracle, and the fallback shows in dol_last_engine() / dol_last_error()."""
+    import ctypes as C
+    torch = cuda
+    L = dol.lib()
+    rng = np.random.default_rng(sum(dims) + 77)
+    m = rand_mask(O, rng, dims, 0.02)
+    md = dev(torch, m)
+    bor = dol.init_border(md, dims)
+    want = O.propagate("danielsson", O.border_init(m, dims), dims, 2)
+    wd = dims + (1,) if len(dims) == 2 else dims
+    need = L.dol_danielsson_workspace_size(*wd)
+    assert need > 0
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run(fn, *extra):
+        work = bor.clone()
+        st = fn(*dims, C.c_void_p(work.data_ptr()), 2, *extra, sp)
+        assert st == dol.OK, L.dol_last_error()
+        engine = L.dol_last_engine()
+        note = L.dol_last_error()
+        dol.sync()
+        np.testing.assert_array_equal(work.cpu().numpy(), want)
+        return engine, note
+
+    plain, ws_fn = ((L.dol_danielsson_2d, L.dol_danielsson_2d_ws) if len(dims) == 2
+                    else (L.dol_danielsson_3d, L.dol_danielsson_3d_ws))
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    assert run(ws_fn, C.c_void_p(ws.data_ptr()), C.c_size_t(need))[0] == ENGINE_BLOCKS
+    assert run(plain)[0] == ENGINE_BLOCKS
+    L.dol_set_workspace_limit(C.c_size_t(need // 2))
+    try:
+        engine, note = run(plain)
+        assert engine == ENGINE_SERIAL and b"serial engine" in note and b"dol_set_workspace_limit" in note
+        # the caller's workspace is not subject to the cap
+        assert run(ws_fn, C.c_void_p(ws.data_ptr()), C.c_size_t(need))[0] == ENGINE_BLOCKS
+    finally:
+        L.dol_set_workspace_limit(C.c_size_t(0))
+    # a caller's workspace that is too small is an error, not a silent fallback
+    work = bor.clone()
+    st = ws_fn(*dims, C.c_void_p(work.data_ptr()), 2, C.c_void_p(ws.data_ptr()), C.c_size_t(need - 1), sp)
+    assert st == dol.ERR_INVALID_ARG and b"workspace too small" in L.dol_last_error()

@@ -402,6 +402,22 @@ def occlusion_sweep_io(dirw_in, dirw_out, dims, stream=None):
     return dirw_out
 
 
+def voxelize(indices, vertices, bbox, dims, mask=None, stream=None):
+    """CreateBitMaskFromTriangles: ORs the cells the triangles touch into `mask`
+    (int32 words on the device; a zeroed mask by default).  indices: int32
+    (t, 3) device tensor or None; vertices: float32 (n, 3) device tensor;
+    bbox: six floats (min xyz, max xyz)."""
+    torch = _torch()
+    w, h, d = _dims(dims)
+    if mask is None:
+        mask = torch.zeros(mask_words(w, h, d), dtype=torch.int32, device=vertices.device)
+    bb = (C.c_float * 6)(*[float(v) for v in bbox])
+    tris = int(indices.shape[0]) if indices is not None else int(vertices.shape[0]) // 3
+    check(lib().dol_voxelize_triangles(C.c_int(tris), _ptr(indices), _ptr(vertices), bb, *_ints(w, h, d),
+                                       _ptr(mask), _stream(stream)))
+    return mask
+
+
 def gen_sites(n, dims, seed):
     """n float sites uniform in continuous cell coordinates, from the reference's
     LCG (24-bit fractions, drawn x, y[, z] per site); float32 array (n, dim)."""

@@ -689,6 +689,28 @@ dol_status dol_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float
     return launched("occlusion_sweep_3d_io");
 }
 
+// ---- mesh voxeliser -------------------------------------------------------------------------------
+
+dol_status dol_voxelize_triangles(int tri_count, const int* indices, const float* vertices, const float* bbox, int w,
+                                  int h, int d, uint32_t* mask, void* stream)
+{
+    DeviceState* ds;
+    DOL_TRY(device_state(&ds));
+    DOL_TRY(check_dims(w, h, d));
+    if (tri_count < 0) return fail(DOL_ERR_INVALID_ARG, "negative triangle count");
+    if (!bbox) return fail(DOL_ERR_INVALID_ARG, "bbox is NULL");
+    for (int i = 0; i < 3; i++)
+        if (!(bbox[3 + i] > bbox[i]))   // also rejects NaN
+            return fail(DOL_ERR_INVALID_ARG, "bbox extent %d is not positive (%g .. %g)", i, bbox[i], bbox[3 + i]);
+    DOL_TRY(check_dev_ptr(mask, "mask"));
+    if (tri_count > 0) {
+        DOL_TRY(check_dev_ptr(vertices, "vertices"));
+        if (indices) DOL_TRY(check_dev_ptr(indices, "indices"));
+    }
+    launch_voxelize(tri_count, indices, vertices, bbox, w, h, d, mask, S(stream));
+    return launched("voxelize_triangles");
+}
+
 // ---- one-call signed fields ----------------------------------------------------------------------
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }

@@ -130,6 +130,10 @@ void launch_init_distances_int(const uint32_t* mask, T* dist, int w, long long r
 void launch_init_dirw(int dim, const uint32_t* mask, float* dirw, int w, int h, int d, cudaStream_t st);
 void launch_occlusion_sweep(int dim, float* dirw, const float* in, int w, int h, int d, cudaStream_t st);
 
+// k_voxel.cu -- triangles to bitmask (ORed into mask); bbox: min xyz, max xyz (host)
+void launch_voxelize(int tri_count, const int* indices, const float* verts, const float bbox[6], int w, int h, int d,
+                     uint32_t* mask, cudaStream_t st);
+
 // k_sites.cu
 void launch_sites_seed(int dim, int w, int h, int d, int n, const float* sites, uint32_t* mask, int* cell_site,
                        cudaStream_t st);

@@ -218,6 +218,17 @@ DOL_API dol_status dol_occlusion_sweep_2d(int w, int h, float* dirW, void* strea
 DOL_API dol_status dol_occlusion_sweep_3d(int w, int h, int d, float* dirW, void* stream);
 DOL_API dol_status dol_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out, void* stream);
 
+/* ---- mesh voxeliser ----------------------------------------------------------------------
+   MSL::CreateBitMaskFromTriangles (MeshSupport.cpp:369-475): ORs into `mask`
+   (device, w x h x d) every cell of the grid spanning `bbox` (HOST array: min
+   x, y, z, max x, y, z) that one of the triangles touches, bit for bit as the
+   reference decides it.  indices: device int[3 * tri_count] into vertices
+   (device float[3 * n]); NULL takes the vertices three per triangle.  Every
+   bbox extent must be positive.  The mask feeds dol_init_border_3d,
+   dol_sdf_3d, dol_edt_mask_3d ... without leaving the device. */
+DOL_API dol_status dol_voxelize_triangles(int tri_count, const int* indices, const float* vertices, const float* bbox,
+                                          int w, int h, int d, uint32_t* mask, void* stream);
+
 /* ---- one-call fields (the tool's Generate* paths) ----------------------------------- */
 /* Signed border-initialised distance field (GenerateSignedDistanceBorder,
    DistanceOcclusionTool.cpp:1333-1365 / :1471-1498): border init, `method`

@@ -1019,3 +1019,142 @@ void dolo_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out
     size_t n = (size_t)w * h * d;
     for (int s = 0; s < 8; s++) occ_plane(w, h, d, s, 3, in + (size_t)s * n, out + (size_t)s * n);
 }
+
+/* ---- mesh voxeliser -----------------------------------------------------------
+ * MSL::CreateBitMaskFromTriangles (MeshSupport.cpp:369-475) with its
+ * triangle / cell overlap tests (cTriCellIntersectDelta, :158-353): for each
+ * triangle, the cells of its bounding box (in the grid spanning bbox) whose
+ * box, grown by 0.000001 of a cell, meets the triangle -- the separating-axis
+ * tests on the edge cross products, the box ranges, then the triangle's
+ * plane -- get their bit set.  Float operations as the reference evaluates
+ * them (this file is built without contraction). */
+typedef struct { float x, y, z; } v3f;
+
+static inline float fmin_ref(float a, float b) { return a < b ? a : b; }
+static inline float fmax_ref(float a, float b) { return b < a ? a : b; }
+
+typedef struct {
+    v3f e[3], t[3], u[3], pmin, pmax, hw, n;
+    float ndv_min, ndv_max, nd;
+} tri_setup;
+
+static void tri_prepare(tri_setup* s, v3f p1, v3f p2, v3f p3, v3f hw)
+{
+    const v3f* P[3] = {&p1, &p2, &p3};
+    s->hw = hw;
+    s->e[0] = (v3f){p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+    s->e[1] = (v3f){p3.x - p2.x, p3.y - p2.y, p3.z - p2.z};
+    s->e[2] = (v3f){p1.x - p3.x, p1.y - p3.y, p1.z - p3.z};
+    /* twice the area normal, :138-150 */
+    s->n.x = (p1.y - p2.y) * (p1.z + p2.z) + (p2.y - p3.y) * (p2.z + p3.z) + (p3.y - p1.y) * (p3.z + p1.z);
+    s->n.y = (p1.z - p2.z) * (p1.x + p2.x) + (p2.z - p3.z) * (p2.x + p3.x) + (p3.z - p1.z) * (p3.x + p1.x);
+    s->n.z = (p1.x - p2.x) * (p1.y + p2.y) + (p2.x - p3.x) * (p2.y + p3.y) + (p3.x - p1.x) * (p3.y + p1.y);
+    v3f vmin = {s->n.x > 0.0f ? -hw.x : hw.x, s->n.y > 0.0f ? -hw.y : hw.y, s->n.z > 0.0f ? -hw.z : hw.z};
+    v3f vmax = {s->n.x > 0.0f ? hw.x : -hw.x, s->n.y > 0.0f ? hw.y : -hw.y, s->n.z > 0.0f ? hw.z : -hw.z};
+    s->ndv_min = s->n.x * vmin.x + s->n.y * vmin.y + s->n.z * vmin.z;
+    s->ndv_max = s->n.x * vmax.x + s->n.y * vmax.y + s->n.z * vmax.z;
+    s->nd = s->n.x * p1.x + s->n.y * p1.y + s->n.z * p1.z;
+    /* per edge k, the vertices its three axis tests project: (for t.x, t.y,
+       t.z) and (for u.x, u.y, u.z), as in :199-239 */
+    static const int tv[3][3] = {{0, 0, 1}, {0, 0, 0}, {0, 0, 1}};
+    static const int uv[3][3] = {{2, 2, 2}, {2, 2, 1}, {1, 1, 2}};
+    for (int k = 0; k < 3; k++) {
+        v3f e = s->e[k];
+        const v3f *a0 = P[tv[k][0]], *a1 = P[tv[k][1]], *a2 = P[tv[k][2]];
+        const v3f *b0 = P[uv[k][0]], *b1 = P[uv[k][1]], *b2 = P[uv[k][2]];
+        v3f t = {e.z * a0->y - e.y * a0->z, -e.z * a1->x + e.x * a1->z, e.y * a2->x - e.x * a2->y};
+        v3f u = {e.z * b0->y - e.y * b0->z, -e.z * b1->x + e.x * b1->z, e.y * b2->x - e.x * b2->y};
+        float q;
+        if (t.x >= u.x) { q = t.x; t.x = u.x; u.x = q; }
+        if (t.y >= u.y) { q = t.y; t.y = u.y; u.y = q; }
+        if (t.z >= u.z) { q = t.z; t.z = u.z; u.z = q; }
+        v3f ae = {fabsf(e.x), fabsf(e.y), fabsf(e.z)};
+        v3f r = {ae.z * hw.y + ae.y * hw.z, ae.z * hw.x + ae.x * hw.z, ae.y * hw.x + ae.x * hw.y};
+        s->t[k] = (v3f){t.x - r.x, t.y - r.y, t.z - r.z};
+        s->u[k] = (v3f){u.x + r.x, u.y + r.y, u.z + r.z};
+    }
+    s->pmin = (v3f){fmin_ref(fmin_ref(p1.x, p2.x), p3.x), fmin_ref(fmin_ref(p1.y, p2.y), p3.y),
+                    fmin_ref(fmin_ref(p1.z, p2.z), p3.z)};
+    s->pmax = (v3f){fmax_ref(fmax_ref(p1.x, p2.x), p3.x), fmax_ref(fmax_ref(p1.y, p2.y), p3.y),
+                    fmax_ref(fmax_ref(p1.z, p2.z), p3.z)};
+}
+
+static int tri_hits_slice(const tri_setup* s, v3f c)
+{
+    return !(s->pmin.z - c.z > s->hw.z || s->pmax.z - c.z < -s->hw.z);
+}
+
+static int tri_hits_row(const tri_setup* s, v3f c)
+{
+    for (int k = 0; k < 3; k++) {
+        float dr = s->e[k].z * c.y - s->e[k].y * c.z;
+        if (s->t[k].x > dr || s->u[k].x < dr) return 0;
+    }
+    return !(s->pmin.y - c.y > s->hw.y || s->pmax.y - c.y < -s->hw.y);
+}
+
+static int tri_hits_cell(const tri_setup* s, v3f c)
+{
+    for (int k = 0; k < 3; k++) {
+        float dr = -s->e[k].z * c.x + s->e[k].x * c.z;
+        if (s->t[k].y > dr || s->u[k].y < dr) return 0;
+        dr = s->e[k].y * c.x - s->e[k].x * c.y;
+        if (s->t[k].z > dr || s->u[k].z < dr) return 0;
+    }
+    if (s->pmin.x - c.x > s->hw.x || s->pmax.x - c.x < -s->hw.x) return 0;
+    float d = s->nd - (s->n.x * c.x + s->n.y * c.y + s->n.z * c.z);
+    return s->ndv_min <= d && s->ndv_max >= d;
+}
+
+void dolo_voxelize(int tri_count, const int* indices, const float* vertices, const float* bbox, int w, int h, int d,
+                   uint32_t* mask)
+{
+    const int ws = words_per_row(w);
+    const size_t slice = (size_t)ws * h;
+    const v3f cmin = {bbox[0], bbox[1], bbox[2]};
+    const v3f ext = {bbox[3] - bbox[0], bbox[4] - bbox[1], bbox[5] - bbox[2]};
+    const v3f cellW = {ext.x / (float)w, ext.y / (float)h, ext.z / (float)d};
+    const v3f inv = {(float)w / ext.x, (float)h / ext.y, (float)d / ext.z};
+    const v3f hw = {cellW.x * 0.500001f, cellW.y * 0.500001f, cellW.z * 0.500001f};
+    for (int t = 0; t < tri_count; t++) {
+        v3f p[3];
+        for (int k = 0; k < 3; k++) {
+            const float* v = vertices + 3 * (size_t)(indices ? indices[3 * t + k] : 3 * t + k);
+            p[k] = (v3f){v[0], v[1], v[2]};
+        }
+        v3f bmin = {fmin_ref(fmin_ref(p[0].x, p[1].x), p[2].x), fmin_ref(fmin_ref(p[0].y, p[1].y), p[2].y),
+                    fmin_ref(fmin_ref(p[0].z, p[1].z), p[2].z)};
+        v3f bmax = {fmax_ref(fmax_ref(p[0].x, p[1].x), p[2].x), fmax_ref(fmax_ref(p[0].y, p[1].y), p[2].y),
+                    fmax_ref(fmax_ref(p[0].z, p[1].z), p[2].z)};
+        int x0 = (int)floorf((bmin.x - cmin.x) * inv.x), y0 = (int)floorf((bmin.y - cmin.y) * inv.y),
+            z0 = (int)floorf((bmin.z - cmin.z) * inv.z);
+        int x1 = (int)ceilf((bmax.x - cmin.x) * inv.x), y1 = (int)ceilf((bmax.y - cmin.y) * inv.y),
+            z1 = (int)ceilf((bmax.z - cmin.z) * inv.z);
+        if (x0 < 0) x0 = 0;
+        if (y0 < 0) y0 = 0;
+        if (z0 < 0) z0 = 0;
+        if (x1 > w) x1 = w;
+        if (y1 > h) y1 = h;
+        if (z1 > d) z1 = d;
+        if (x0 == x1) continue;   /* as the reference: only an empty x range skips the triangle */
+        if (x0 + 1 == x1 && y0 + 1 == y1 && z0 + 1 == z1) {   /* a single cell: set without testing */
+            mask[slice * z0 + (size_t)ws * y0 + (x0 >> 5)] |= 1u << (x0 & 31);
+            continue;
+        }
+        tri_setup s;
+        tri_prepare(&s, p[0], p[1], p[2], hw);
+        for (int z = z0; z < z1; z++) {
+            v3f c;
+            c.z = cmin.z + cellW.z * ((float)z + 0.5f);
+            if (!tri_hits_slice(&s, c)) continue;
+            for (int y = y0; y < y1; y++) {
+                c.y = cmin.y + cellW.y * ((float)y + 0.5f);
+                if (!tri_hits_row(&s, c)) continue;
+                for (int x = x0; x < x1; x++) {
+                    c.x = cmin.x + cellW.x * ((float)x + 0.5f);
+                    if (tri_hits_cell(&s, c)) mask[slice * z + (size_t)ws * y + (x >> 5)] |= 1u << (x & 31);
+                }
+            }
+        }
+    }
+}

@@ -93,6 +93,12 @@ void dolo_occlusion_sweep_2d(int w, int h, float* dirW);
 void dolo_occlusion_sweep_3d(int w, int h, int d, float* dirW);
 void dolo_occlusion_sweep_3d_io(int w, int h, int d, const float* in, float* out);
 
+/* mesh voxeliser: ORs the cells of the w x h x d grid over bbox (min xyz, max
+   xyz) that the triangles touch into mask; indices may be NULL (vertices then
+   taken three per triangle) */
+void dolo_voxelize(int tri_count, const int* indices, const float* vertices, const float* bbox, int w, int h, int d,
+                   uint32_t* mask);
+
 #ifdef __cplusplus
 }
 #endif

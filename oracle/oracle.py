@@ -359,3 +359,53 @@ def occlusion_sweep_io(dirw_in, dirw_out, dims, use_ref=False):
     pre, L = ("ref_", ref()) if use_ref else ("dolo_", lib())
     getattr(L, pre + "occlusion_sweep_3d_io")(*_i(*dims), _p(src), _p(out))
     return out
+
+
+# ---- mesh voxeliser ------------------------------------------------------------------------
+
+def load_tri(path):
+    """A triangle file written by oracle/_ref/mesh_dump: (indices int32[t, 3],
+    vertices float32[v, 3], bbox float32[6])."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    nt, nv = np.frombuffer(raw[:8].tobytes(), np.int32)
+    bbox = np.frombuffer(raw[8:32].tobytes(), np.float32).copy()
+    o = 32
+    verts = np.frombuffer(raw[o:o + 12 * nv].tobytes(), np.float32).reshape(nv, 3).copy()
+    o += 12 * nv
+    idx = np.frombuffer(raw[o:o + 12 * nt].tobytes(), np.int32).reshape(nt, 3).copy()
+    return idx, verts, bbox
+
+
+def voxelize(indices, vertices, bbox, dims, mask=None, use_ref=False):
+    """CreateBitMaskFromTriangles: ORs the touched cells into `mask` (a fresh
+    zero mask by default); returns the mask."""
+    w, h, d = dims
+    m = new_mask(w, h, d) if mask is None else mask.copy()
+    idx = np.ascontiguousarray(indices, np.int32)
+    v = np.ascontiguousarray(vertices, np.float32)
+    bb = np.ascontiguousarray(bbox, np.float32)
+    if use_ref:
+        ref().ref_voxelize(C.c_int(idx.shape[0]), _p(idx), _p(v), _p(bb), *_i(w, h, d), _p(m))
+    else:
+        lib().dolo_voxelize(C.c_int(idx.shape[0]), _p(idx), _p(v), _p(bb), *_i(w, h, d), _p(m))
+    return m
+
+
+def random_triangles(rng, n, scale=(0.002, 0.3), nverts=None):
+    """A soup of n triangles in the unit cube: sizes log-uniform in `scale`,
+    some degenerate (repeated or collinear vertices); returns (indices,
+    vertices, bbox) with bbox the vertices' bounds."""
+    c = rng.random((n, 1, 3))
+    size = np.exp(rng.uniform(np.log(scale[0]), np.log(scale[1]), (n, 1, 1)))
+    tri = c + (rng.random((n, 3, 3)) - 0.5) * size
+    k = max(1, n // 40)
+    tri[:k, 2] = tri[:k, 1]                                        # repeated vertex
+    tri[k:2 * k, 2] = 2 * tri[k:2 * k, 1] - tri[k:2 * k, 0]          # collinear
+    verts = tri.reshape(-1, 3).astype(np.float32)
+    idx = np.arange(3 * n, dtype=np.int32).reshape(n, 3)
+    perm = rng.permutation(3 * n).astype(np.int32)                # shuffled vertex order, indexed
+    vs = np.empty_like(verts)
+    vs[perm] = verts
+    idx = perm[idx]
+    bbox = np.concatenate([verts.min(0), verts.max(0)]).astype(np.float32)
+    return idx, vs, bbox

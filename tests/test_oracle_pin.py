@@ -294,3 +294,28 @@ def test_occlusion_matches_reference(O, dims):
             got = O.occlusion_sweep_io(dw, prior, dims)
             want = O.occlusion_sweep_io(dw, prior, dims, use_ref=True)
             np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=f"io {dims} p={p}")
+
+
+# ---- mesh voxeliser -------------------------------------------------------------------------
+
+def _tri_file():
+    return os.path.join(os.path.dirname(HERE), "oracle", "_ref", "plant2.tri")
+
+
+@pytest.mark.parametrize("dims", [(32, 32, 32), (64, 64, 64), (100, 80, 60), (33, 17, 70)])
+def test_voxelize_matches_reference(O, dims):
+    if O.ref() is None:
+        pytest.skip("reference build (oracle/_ref) absent")
+    rng = np.random.default_rng(sum(dims))
+    cases = [O.random_triangles(rng, 400), O.random_triangles(rng, 50, scale=(0.3, 1.5))]
+    if os.path.exists(_tri_file()):
+        cases.append(O.load_tri(_tri_file()))
+    for idx, v, bb in cases:
+        got = O.voxelize(idx, v, bb, dims)
+        want = O.voxelize(idx, v, bb, dims, use_ref=True)
+        np.testing.assert_array_equal(got, want)
+        assert want.any()
+        # ORs into what the mask already holds
+        prior = O.bool_to_mask(rng.random(tuple(reversed(dims))) < 0.01)
+        np.testing.assert_array_equal(O.voxelize(idx, v, bb, dims, mask=prior),
+                                      O.voxelize(idx, v, bb, dims, mask=prior, use_ref=True))

@@ -819,6 +819,107 @@ def danielsson_only(shape):
     print(json.dumps({"danielsson_signed": shape, "ms": times}), flush=True)
 
 
+# ------------------------------------------------------------ single kernels ----
+# One small workload per kernel family, run `reps` times after one untimed run,
+# each timed with CUDA events: the commands the ncu summaries under profiles/
+# are made with (inputs larger than L2 where the family allows, a few GB at
+# most on the device).
+
+def _case_inputs(dol, torch, L, kind, n):
+    dims = (n, n, n)
+    md = torch.empty(dol.mask_words(*dims), dtype=torch.int32, device="cuda")
+    if kind == "noise":
+        dol.check(L.dol_gen_value_noise_3d(n, n, n, SPACING, C.c_uint32(SEED), C.c_void_p(md.data_ptr()), None))
+    elif kind == "shapes":
+        dol.check(L.dol_gen_shapes_3d(n, n, n, 32 * n // 256, 32 * n // 256, 4 * n // 256, 40 * n // 256,
+                                      C.c_uint32(7), C.c_void_p(md.data_ptr()), None))
+    else:   # 2000 points per 1024^3, scaled
+        mh = np.zeros(dol.mask_words(*dims), np.uint32)
+        md = torch.from_numpy(dol.add_points(mh, dims, max(1, 2000 * n ** 3 // 1024 ** 3), 1).view(np.int32)).cuda()
+    return dims, md
+
+
+def run_case(name, reps=2):
+    import torch
+    dol = load_dol()
+    L = dol.lib()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    fn, note = None, ""
+    if name.startswith("edt_"):                    # edt_noise_512, edt_points_512, edt_shapes_256
+        _, kind, n = name.split("_")
+        dims, md = _case_inputs(dol, torch, L, kind, int(n))
+        out = dol.empty_field(dims)
+        ws = torch.empty(L.dol_edt_mask_3d_workspace_size(*dims), dtype=torch.uint8, device="cuda")
+        fn = lambda: dol.edt_mask(md, dims, dol.EDT_SIGNED, out=out, workspace=ws)
+    elif name in ("border_256", "danielsson_256", "fastsweep_256", "jumpflood_256", "dist_256"):
+        dims, md = _case_inputs(dol, torch, L, "shapes", 256)
+        bor = dol.init_border(md, dims)
+        work = bor.clone()
+        f = dol.empty_field(dims)
+        meth = name.split("_")[0]
+        if meth == "border":
+            fn = lambda: dol.init_border(md, dims, out=work)
+        elif meth == "dist":
+            dol.danielsson(work, dims, 2)
+            fn = lambda: dol.check(L.dol_deltas_to_dist_3d(*dims, C.c_void_p(work.data_ptr()), 2,
+                                                            C.c_void_p(md.data_ptr()), C.c_void_p(f.data_ptr()), None))
+        else:
+            def fn(meth=meth):
+                work.copy_(bor)
+                dol.propagate(meth, work, dims, 2)
+    elif name == "chamfer_1024":
+        dims = (1024, 1024)
+        m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+        md = torch.from_numpy(m.view(np.int32)).cuda()
+        f0 = dol.init_distances_int(md, dims, "int16", 32767 - 16)
+        f = f0.clone()
+
+        def fn():
+            f.copy_(f0)
+            dol.chamfer(f, dims)
+    elif name in ("occlusion_1024", "occlusion_128"):
+        n = int(name.split("_")[1])
+        if n == 1024:
+            dims = (1024, 1024)
+            md = torch.from_numpy(dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+                                  .view(np.int32)).cuda()
+        else:
+            dims, md = _case_inputs(dol, torch, L, "noise", n)
+        dw = dol.init_dirw(md, dims)
+        fn = lambda: dol.occlusion_sweep(dol.init_dirw(md, dims, out=dw), dims)
+    elif name.startswith("voxel_"):                # voxel_256: the reference's sample mesh
+        import oracle as O
+        n = int(name.split("_")[1])
+        idx, v, bb = O.load_tri(os.path.join(ROOT, "oracle", "_ref", "plant2.tri"))
+        it, vt = torch.from_numpy(idx).cuda(), torch.from_numpy(v).cuda()
+        m = torch.zeros(dol.mask_words(n, n, n), dtype=torch.int32, device="cuda")
+        fn = lambda: dol.voxelize(it, vt, bb, (n, n, n), mask=m)
+    elif name == "batch":
+        res = {}
+        _config4(dol, torch, res, L, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        print(json.dumps({"case": name, **res["batch_4096_64"]}), flush=True)
+        return
+    elif name.startswith("sites_"):                # sites_512: 4096 sites, Danielsson forward + backward
+        dims = (512, 512)
+        s = torch.from_numpy(dol.gen_sites(4096, dims, 11)).cuda()
+
+        def fn():
+            d, own, _ = dol.sites_forward(s, dims, "danielsson")
+            dol.sites_backward(own, s, 2.0 * d, dims)
+    else:
+        raise SystemExit(f"unknown case {name}")
+    fn()
+    torch.cuda.synchronize()
+    ms = [_ev_ms(torch, fn, 1) for _ in range(reps)]
+    dol.sync()
+    print(json.dumps({"case": name, "ms": ms, "note": note}), flush=True)
+
+
+CASES = ["edt_noise_512", "edt_points_512", "edt_shapes_256", "border_256", "danielsson_256", "fastsweep_256",
+         "jumpflood_256", "dist_256", "chamfer_1024", "occlusion_1024", "occlusion_128", "voxel_256", "batch",
+         "sites_512"]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -835,6 +936,7 @@ def main():
     ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
     ap.add_argument("--only", default=None,
                     help="comma list of c1..c7: run only these per-configuration measurements (no headline)")
+    ap.add_argument("--case", default=None, choices=CASES, help="run one kernel family's small workload (profiling)")
     ap.add_argument("--danielsson", default=None, metavar="WxHxD",
                     help="only time signed Danielsson on a WxHxD value-noise volume (twice; for profiling)")
     args = ap.parse_args()
@@ -842,6 +944,8 @@ def main():
     W = H = D = args.side
     if args.impl == "reference":
         run_reference(args)
+    elif args.case:
+        run_case(args.case)
     elif args.danielsson:
         danielsson_only(args.danielsson)
     elif args.only:

@@ -474,6 +474,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     TIn* F0 = reinterpret_cast<TIn*>(smem_raw) + kPadRows * TX;   // rows -kPadRows .. rows+kPadRows-1, first the raw tile
     TIn* F1 = F0 + (rows + 2 * kPadRows) * TX;                      // the same for state 1
     __shared__ __align__(8) uint64_t bar;
+    __shared__ unsigned s_score;   // far cells of the tile (envelope-path test)
     int x0, outer, line = 0;
     if (kMode == 2) {
         // one block per (y, 8-column group) of the [y][x/8][z][8] array
@@ -485,7 +486,10 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         x0 = blockIdx.x * TX;
         outer = blockIdx.y + outer0;
     }
-    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        s_score = 0;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_expect_tx(&bar, (uint32_t)(rows * TX * sizeof(TIn)));
@@ -512,13 +516,19 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     uint4* V1 = reinterpret_cast<uint4*>(F1);
     const uint32_t sw = sizeof(TIn) == 2 ? 0x7FFF7FFFu : 0x7FFFFFFFu;   // a word of sentinels / value bits
     const uint4 sent = make_uint4(sw, sw, sw, sw);
-    // while splitting, note any own value above the window threshold (a
-    // distance above hull_thr; "none" counts): such a tile takes the envelope path
-    const uint32_t thr = sizeof(TIn) == 2 ? (hull_thr > 0x7FFFu ? 0x7FFFu : hull_thr) * 0x00010001u
-                                          : (hull_thr >= 46341u ? 0x7FFFFFFFu : hull_thr * hull_thr);
-    uint32_t big = 0;
-    auto over = [&](uint32_t x) -> uint32_t {
-        return sizeof(TIn) == 2 ? __vcmpgtu2(x & sw, thr) : (uint32_t)((x & sw) > thr);
+    // while splitting, count the cells whose own value (their distance to the
+    // other state in the lower dimensions) exceeds the window threshold
+    // hull_thr, a cell with none counting 16 times (its walk would run to the
+    // line end): when they make up a quarter of the tile, it takes the
+    // envelope path.  Dense fields have few such cells, sparse ones mostly.
+    const uint32_t thr = sizeof(TIn) == 2 ? (hull_thr > 0x7FFEu ? 0x7FFEu : hull_thr) * 0x00010001u
+                                          : (hull_thr >= 46341u ? 0x7FFFFFFEu : hull_thr * hull_thr);
+    uint32_t score = 0;
+    auto weigh = [&](uint32_t x) -> uint32_t {
+        const uint32_t v = x & sw;
+        if (sizeof(TIn) == 2)
+            return (__popc(__vcmpgtu2(v, thr)) + 15 * __popc(__vcmpeq2(v, sw))) >> 4;
+        return (v > thr ? 1u : 0u) + (v == sw ? 15u : 0u);
     };
     for (int i = threadIdx.x; i < n * kVecRow; i += blockDim.x) {
         const uint4 x = V0[i];
@@ -529,7 +539,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         split_word<TIn>(x.w, sw, &a.w, &b.w);
         V0[i] = a;
         V1[i] = b;
-        big |= over(x.x) | over(x.y) | over(x.z) | over(x.w);
+        score += weigh(x.x) + weigh(x.y) + weigh(x.z) + weigh(x.w);
     }
     for (int i = n * kVecRow + threadIdx.x; i < (rows + kPadRows) * kVecRow; i += blockDim.x) {
         V0[i] = sent;
@@ -539,7 +549,11 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         V0[i - kPadRows * kVecRow] = sent;
         V1[i - kPadRows * kVecRow] = sent;
     }
-    const bool use_hull = __syncthreads_or(big != 0 && hull_thr != 0xFFFFFFFFu);
+    score = __reduce_add_sync(0xFFFFFFFFu, score);
+    if ((threadIdx.x & 31) == 0 && score) atomicAdd(&s_score, score);
+    __syncthreads();
+    const long long tile_cells = (long long)n * min(TX, w - x0);
+    const bool use_hull = hull_thr == 0u || (hull_thr != 0xFFFFFFFFu && 4LL * s_score > tile_cells);
 
     if (use_hull) {
         // envelope path: units (column, 32-cell segment); hull words after the tile
@@ -712,9 +726,10 @@ static bool blocked_layout_ok(const uint16_t* vx, const uint32_t* ey, int w, int
     return line_map<uint16_t, 16>(&m, vx, w, h, d, 0, 1) && line_map<uint32_t, 8>(&m, ey, w, h, d, 1, 2);
 }
 
-// Window threshold of the line passes: a tile holding an own value (a cell's
-// distance to the other state in the lower dimensions) above it takes the
-// envelope path.  The tuned value (DOL_TUNE_EDT_HULL, by line length): 1 =
+// Window threshold of the line passes: a tile where a quarter of the cells
+// (a cell with no other-state cell on its lower-dimension lines counting 16)
+// lie farther than this from the other state in the lower dimensions takes
+// the envelope path.  The tuned value (DOL_TUNE_EDT_HULL, by line length): 1 =
 // windowed search only, 2 = envelope only, >= 3 = that distance; 0 = 24.
 static uint32_t edt_hull_threshold(int n)
 {

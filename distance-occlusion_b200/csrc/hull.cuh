@@ -194,13 +194,17 @@ template <typename TIn, class Emit>
 DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
                        Emit&& emit)
 {
-    int v0 = -2, v1 = -2;   // per state: current vertex, -2 = not placed yet, -1 = empty hull
+    // per state: the current vertex c (-2 = not placed yet, -1 = empty hull)
+    // and the vertex after it r (-2 = not looked up, -1 = none): c only moves
+    // right, so r stays valid until c moves, and the scan over empty hull
+    // words to find it is done once per move, not once per cell
+    int c0 = -2, c1 = -2, r0 = -2, r1 = -2;
     const int p0 = seg << 5, p1 = n < p0 + 32 ? n : p0 + 32;
     for (int p = p0; p < p1; p++) {
         const int s = F1[p * TXv + col] != 0;
         const TIn* Fs = s ? F1 : F0;
         const uint32_t* W = HM + (s * TXv + col) * nseg;
-        int c = s ? v1 : v0;
+        int c = s ? c1 : c0, r = s ? r1 : r0;
         if (c == -2) {   // first cell of this state in the unit: place the pointer
             // the first vertex at or after p, else the last one before it
             if (p == 0)
@@ -219,23 +223,27 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
                     cv = lv;
                 }
             }
+            r = -2;
         }
         uint32_t best = 0xFFFFFFFFu;
         if (c >= 0) {
             best = hull_at<TIn>(Fs, c, p, TXv, col);
-            for (;;) {   // and to the right, as p advances
-                const int r = hull_next(W, c, nseg);
-                if (r < 0) break;
+            if (r == -2) r = hull_next(W, c, nseg);
+            while (r >= 0) {   // and to the right, as p advances
                 const uint32_t rv = hull_at<TIn>(Fs, r, p, TXv, col);
                 if (rv > best) break;
                 c = r;
                 best = rv;
+                r = hull_next(W, c, nseg);
             }
         }
-        if (s)
-            v1 = c;
-        else
-            v0 = c;
+        if (s) {
+            c1 = c;
+            r1 = r;
+        } else {
+            c0 = c;
+            r0 = r;
+        }
         emit(p, s, best, c < 0);
     }
 }

@@ -86,10 +86,11 @@ DOL_HD int hull_prev(const uint32_t* W, int v, int lo)
     return (wi << 5) + hibit32(m);
 }
 
-// Segment hulls of both transforms for unit (col, seg) of a line of n cells,
-// written to HM[(s * TXv + col) * nseg + seg].
+// Segment hulls of both transforms (or of transform s_only) for unit (col,
+// seg) of a line of n cells, written to HM[(s * TXv + col) * nseg + seg].
 template <typename TIn>
-DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int nseg, int n, int col, int seg)
+DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
+                       int s_only = -1)
 {
     const int p0 = seg << 5;
     const uint32_t sent = sizeof(TIn) == 2 ? 0x7FFFu : 0x7FFFFFFFu;
@@ -106,6 +107,7 @@ DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int 
     const uint32_t s_prev = pv ? (uint32_t)(F1[(p0 - 1) * TXv + col] != 0) : 0u;
     const uint32_t s_next = nx ? (uint32_t)(F1[(p0 + 32) * TXv + col] != 0) : 0u;
     for (int s = 0; s < 2; s++) {
+        if (s_only >= 0 && s != s_only) continue;   // the other transform is another thread's
         const TIn* Fs = s ? F1 : F0;
         const uint32_t own = (s ? S : ~S) & live;
         const uint32_t other = (s ? ~S : S) & live;
@@ -180,6 +182,22 @@ DOL_HD void hull_merge(const TIn* Fs, uint32_t* W, int TXv, int col, int lo, int
     }
 }
 
+// The whole merge tree of one (state, column)'s hull words: at each level,
+// pair g of segment groups is merged by the caller's thread `g mod lanes`;
+// `sync` runs between levels (a warp barrier on the device).
+template <typename TIn, class Sync>
+DOL_HD void hull_merge_tree(const TIn* Fs, uint32_t* W, int TXv, int col, int nseg, int lane, int lanes, Sync&& sync)
+{
+    for (int half = 1; half < nseg; half <<= 1) {
+        const int groups = (nseg + 2 * half - 1) / (2 * half);
+        for (int g = lane; g < groups; g += lanes) {
+            const int lo = g * 2 * half, mid = lo + half, hi = mid + half < nseg ? mid + half : nseg;
+            if (mid < nseg) hull_merge<TIn>(Fs, W, TXv, col, lo, mid, hi);
+        }
+        sync();
+    }
+}
+
 // value of hull vertex v at position p: G(v) + (p - v)^2
 template <typename TIn>
 DOL_HD uint32_t hull_at(const TIn* Fs, int v, int p, int TXv, int col)
@@ -188,11 +206,12 @@ DOL_HD uint32_t hull_at(const TIn* Fs, int v, int p, int TXv, int col)
     return sq_val<TIn>(Fs[v * TXv + col]) + (uint32_t)(d * d);
 }
 
-// The cells of unit (col, seg) against the merged hulls: emit(p, s, best,
-// none) per cell p < n, best = the transform's value (meaningless if none).
+// The cells of unit (col, seg) (of state s_only, when given) against the
+// merged hulls: emit(p, s, best, none) per cell p < n, best = the
+// transform's value (meaningless if none).
 template <typename TIn, class Emit>
 DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
-                       Emit&& emit)
+                       Emit&& emit, int s_only = -1)
 {
     // per state: the current vertex c (-2 = not placed yet, -1 = empty hull)
     // and the vertex after it r (-2 = not looked up, -1 = none): c only moves
@@ -202,6 +221,7 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
     const int p0 = seg << 5, p1 = n < p0 + 32 ? n : p0 + 32;
     for (int p = p0; p < p1; p++) {
         const int s = F1[p * TXv + col] != 0;
+        if (s_only >= 0 && s != s_only) continue;   // another thread's cell
         const TIn* Fs = s ? F1 : F0;
         const uint32_t* W = HM + (s * TXv + col) * nseg;
         int c = s ? c1 : c0, r = s ? r1 : r0;

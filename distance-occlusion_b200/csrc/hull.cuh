@@ -22,7 +22,7 @@
 // (the lower bridge of two x-separated hulls, walked from their facing ends,
 // clearing the vertices it passes); each unit then walks its cells left to
 // right with one pointer per state.  Arithmetic is exact: points in 64 bits,
-// orientation by cross products of at most ~2^46.
+// orientation by cross products of 32-bit differences (at most ~2^45).
 //
 // Arrays: Fs points at position 0 of one state's split array, rows of TXv
 // elements (column col at offset col); positions up to the segment-rounded
@@ -50,17 +50,20 @@ DOL_HD uint32_t sq_val(TIn v)
     return sizeof(TIn) == 2 ? (uint32_t)v * (uint32_t)v : (uint32_t)v;
 }
 
-// hull y of position p in transform s: G_s(p) + p^2
+// hull y of position p in transform s: G_s(p) + p^2.  Below 2^31 for every
+// supported size: a candidate's G is at most (16383^2) * 2 < 2^29 and
+// p^2 < 2^28, so points and their differences fit 32 bits.
 template <typename TIn>
-DOL_HD long long hull_y(const TIn* Fs, int p, int TXv, int col)
+DOL_HD int hull_y(const TIn* Fs, int p, int TXv, int col)
 {
-    return (long long)sq_val<TIn>(Fs[p * TXv + col]) + (long long)p * p;
+    return (int)(sq_val<TIn>(Fs[p * TXv + col]) + (uint32_t)(p * p));
 }
 
-// true iff (xb, yb) lies strictly below the segment from (xa, ya) to (xc, yc), xa < xb < xc
-DOL_HD bool hull_keep(int xa, long long ya, int xb, long long yb, int xc, long long yc)
+// true iff (xb, yb) lies strictly below the segment from (xa, ya) to (xc, yc),
+// xa < xb < xc: two 32 x 32 -> 64-bit products, exact
+DOL_HD bool hull_keep(int xa, int ya, int xb, int yb, int xc, int yc)
 {
-    return (long long)(xb - xa) * (yc - ya) - (long long)(xc - xa) * (yb - ya) > 0;
+    return (long long)(xb - xa) * (long long)(yc - ya) - (long long)(xc - xa) * (long long)(yb - ya) > 0;
 }
 
 // nearest vertex after v in words [.., hi) / before v in words [lo, ..); -1 if none
@@ -86,17 +89,18 @@ DOL_HD int hull_prev(const uint32_t* W, int v, int lo)
     return (wi << 5) + hibit32(m);
 }
 
-// Segment hulls of both transforms (or of transform s_only) for unit (col,
-// seg) of a line of n cells, written to HM[(s * TXv + col) * nseg + seg].
+// Segment hulls of both transforms for unit (col, seg) of a line of n cells,
+// written to HM[(s * TXv + col) * nseg + seg].
 template <typename TIn>
-DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
-                       int s_only = -1)
+DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int nseg, int n, int col, int seg)
 {
     const int p0 = seg << 5;
     const uint32_t sent = sizeof(TIn) == 2 ? 0x7FFFu : 0x7FFFFFFFu;
     uint32_t S = 0, inf = 0;   // state bits; own value "none"
-    for (int t = 0; t < 32; t++) {
-        const int p = p0 + t;
+    for (int i = 0; i < 32; i++) {
+        // rotated by the segment: the units of a warp, in consecutive
+        // segments, then read rows in different shared-memory banks
+        const int t = (i + seg) & 31, p = p0 + t;
         const uint32_t r0 = F0[p * TXv + col], r1 = F1[p * TXv + col];
         S |= (uint32_t)(r1 != 0) << t;
         inf |= (uint32_t)((r0 | r1) == sent) << t;
@@ -107,7 +111,6 @@ DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int 
     const uint32_t s_prev = pv ? (uint32_t)(F1[(p0 - 1) * TXv + col] != 0) : 0u;
     const uint32_t s_next = nx ? (uint32_t)(F1[(p0 + 32) * TXv + col] != 0) : 0u;
     for (int s = 0; s < 2; s++) {
-        if (s_only >= 0 && s != s_only) continue;   // the other transform is another thread's
         const TIn* Fs = s ? F1 : F0;
         const uint32_t own = (s ? S : ~S) & live;
         const uint32_t other = (s ? ~S : S) & live;
@@ -117,12 +120,12 @@ DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int 
         uint32_t cand = (own & ~inf) | (other & near_own);
         uint32_t M = 0;
         int xa = -1, xb = -1;
-        long long ya = 0, yb = 0;
+        int ya = 0, yb = 0;
         while (cand) {
             const int t = ffs32(cand);
             cand &= cand - 1;
             const int p = p0 + t;
-            const long long yc = hull_y<TIn>(Fs, p, TXv, col);
+            const int yc = hull_y<TIn>(Fs, p, TXv, col);
             while (xa >= 0 && !hull_keep(xa, ya, xb, yb, p, yc)) {
                 M &= ~(1u << (xb - p0));   // pop the top
                 xb = xa;
@@ -156,11 +159,11 @@ DOL_HD void hull_merge(const TIn* Fs, uint32_t* W, int TXv, int col, int lo, int
     for (int i = mid; i < hi && b < 0; i++)
         if (W[i]) b = (i << 5) + ffs32(W[i]);
     if (b < 0) return;
-    long long ya = hull_y<TIn>(Fs, a, TXv, col), yb = hull_y<TIn>(Fs, b, TXv, col);
+    int ya = hull_y<TIn>(Fs, a, TXv, col), yb = hull_y<TIn>(Fs, b, TXv, col);
     for (;;) {
         const int ap = hull_prev(W, a, lo);
         if (ap >= 0) {
-            const long long yp = hull_y<TIn>(Fs, ap, TXv, col);
+            const int yp = hull_y<TIn>(Fs, ap, TXv, col);
             if (!hull_keep(ap, yp, a, ya, b, yb)) {
                 W[a >> 5] &= ~(1u << (a & 31));
                 a = ap;
@@ -170,7 +173,7 @@ DOL_HD void hull_merge(const TIn* Fs, uint32_t* W, int TXv, int col, int lo, int
         }
         const int bn = hull_next(W, b, hi);
         if (bn >= 0) {
-            const long long yn = hull_y<TIn>(Fs, bn, TXv, col);
+            const int yn = hull_y<TIn>(Fs, bn, TXv, col);
             if (!hull_keep(a, ya, b, yb, bn, yn)) {
                 W[b >> 5] &= ~(1u << (b & 31));
                 b = bn;
@@ -182,22 +185,6 @@ DOL_HD void hull_merge(const TIn* Fs, uint32_t* W, int TXv, int col, int lo, int
     }
 }
 
-// The whole merge tree of one (state, column)'s hull words: at each level,
-// pair g of segment groups is merged by the caller's thread `g mod lanes`;
-// `sync` runs between levels (a warp barrier on the device).
-template <typename TIn, class Sync>
-DOL_HD void hull_merge_tree(const TIn* Fs, uint32_t* W, int TXv, int col, int nseg, int lane, int lanes, Sync&& sync)
-{
-    for (int half = 1; half < nseg; half <<= 1) {
-        const int groups = (nseg + 2 * half - 1) / (2 * half);
-        for (int g = lane; g < groups; g += lanes) {
-            const int lo = g * 2 * half, mid = lo + half, hi = mid + half < nseg ? mid + half : nseg;
-            if (mid < nseg) hull_merge<TIn>(Fs, W, TXv, col, lo, mid, hi);
-        }
-        sync();
-    }
-}
-
 // value of hull vertex v at position p: G(v) + (p - v)^2
 template <typename TIn>
 DOL_HD uint32_t hull_at(const TIn* Fs, int v, int p, int TXv, int col)
@@ -206,12 +193,11 @@ DOL_HD uint32_t hull_at(const TIn* Fs, int v, int p, int TXv, int col)
     return sq_val<TIn>(Fs[v * TXv + col]) + (uint32_t)(d * d);
 }
 
-// The cells of unit (col, seg) (of state s_only, when given) against the
-// merged hulls: emit(p, s, best, none) per cell p < n, best = the
-// transform's value (meaningless if none).
+// The cells of unit (col, seg) against the merged hulls: emit(p, s, best,
+// none) per cell p < n, best = the transform's value (meaningless if none).
 template <typename TIn, class Emit>
 DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
-                       Emit&& emit, int s_only = -1)
+                       Emit&& emit)
 {
     // per state: the current vertex c (-2 = not placed yet, -1 = empty hull)
     // and the vertex after it r (-2 = not looked up, -1 = none): c only moves
@@ -221,7 +207,6 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
     const int p0 = seg << 5, p1 = n < p0 + 32 ? n : p0 + 32;
     for (int p = p0; p < p1; p++) {
         const int s = F1[p * TXv + col] != 0;
-        if (s_only >= 0 && s != s_only) continue;   // another thread's cell
         const TIn* Fs = s ? F1 : F0;
         const uint32_t* W = HM + (s * TXv + col) * nseg;
         int c = s ? c1 : c0, r = s ? r1 : r0;

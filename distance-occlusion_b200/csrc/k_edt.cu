@@ -556,42 +556,37 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     const bool use_hull = hull_thr == 0u || (hull_thr != 0xFFFFFFFFu && 4LL * s_score > tile_cells);
 
     if (use_hull) {
-        // envelope path: units (column, 32-cell segment); hull words after
-        // the tile.  With fewer units than threads, two threads share a unit,
-        // one transform each.
+        // envelope path: units (column, 32-cell segment); hull words after the tile
         const int nseg = (n + 31) >> 5;
         uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
         const int units = TX * nseg;
-        const int ways = units * 2 <= (int)blockDim.x ? 2 : 1;
-        for (int u = threadIdx.x; u < units * ways; u += blockDim.x) {
-            const int uu = u % units, col = uu % TX, seg = uu / TX;
-            if (x0 + col < w) hull_build<TIn>(F0, F1, HM, TX, nseg, n, col, seg, ways == 2 ? u / units : -1);
+        for (int u = threadIdx.x; u < units; u += blockDim.x) {
+            const int col = u % TX, seg = u / TX;
+            if (x0 + col < w) hull_build<TIn>(F0, F1, HM, TX, nseg, n, col, seg);
         }
         __syncthreads();
-        {   // the merge tree of each (state, column), one warp each, warp barriers between levels
-            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-            for (int sc = wid; sc < 2 * TX; sc += nwarps) {
-                const int col = sc % TX;
-                if (x0 + col < w)
-                    hull_merge_tree<TIn>(sc >= TX ? F1 : F0, HM + (size_t)sc * nseg, TX, col, nseg, lane, 32,
-                                         [] { __syncwarp(); });
+        for (int half = 1; half < nseg; half <<= 1) {
+            const int groups = (nseg + 2 * half - 1) / (2 * half);
+            for (int j = threadIdx.x; j < 2 * TX * groups; j += blockDim.x) {
+                const int g = j % groups, sc = j / groups;   // sc = s * TX + col
+                const int col = sc % TX, s = sc / TX;
+                const int lo = g * 2 * half, mid = lo + half, hi = min(mid + half, nseg);
+                if (mid < nseg && x0 + col < w)
+                    hull_merge<TIn>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
             }
+            __syncthreads();
         }
-        __syncthreads();
         const uint32_t kNoneH = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-        for (int u = threadIdx.x; u < units * ways; u += blockDim.x) {
-            const int uu = u % units, col = uu % TX, seg = uu / TX;
+        for (int u = threadIdx.x; u < units; u += blockDim.x) {
+            const int col = u % TX, seg = u / TX;
             const int x = x0 + col;
             if (x >= w) continue;
             const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
                                               : (long long)outer * outer_stride + x;
-            hull_query<TIn>(
-                F0, F1, HM, TX, nseg, n, col, seg,
-                [&](int p, int s, uint32_t best, bool none) {
-                    put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best,
-                                           none || best >= kNoneH, form);
-                },
-                ways == 2 ? u / units : -1);
+            hull_query<TIn>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
+                put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best, none || best >= kNoneH,
+                                       form);
+            });
         }
         return;
     }

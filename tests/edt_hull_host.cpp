@@ -6,57 +6,33 @@
 #include "hull.cuh"
 
 template <typename TIn>
-static void run_tile(int n, int TX, const TIn* F0, const TIn* F1, uint32_t* best, uint8_t* none, int split,
-                     int lanes)
+static void run_tile(int n, int TX, const TIn* F0, const TIn* F1, uint32_t* best, uint8_t* none)
 {
     const int nseg = (n + 31) / 32;
     std::vector<uint32_t> HM(2 * (size_t)TX * nseg);
-    // split != 0: each transform built and answered on its own, as two threads sharing a unit do
     for (int seg = 0; seg < nseg; seg++)
-        for (int col = 0; col < TX; col++) {
-            if (split)
-                for (int s = 0; s < 2; s++) dolk::hull_build<TIn>(F0, F1, HM.data(), TX, nseg, n, col, seg, s);
-            else
-                dolk::hull_build<TIn>(F0, F1, HM.data(), TX, nseg, n, col, seg);
-        }
-    // the merge tree of each (state, column): every lane of a level runs before the next level starts
-    // (one lane: the kernel's own helper)
-    for (int sc = 0; sc < 2 * TX; sc++)
-        if (lanes == 1)
-            dolk::hull_merge_tree<TIn>(sc >= TX ? F1 : F0, HM.data() + (size_t)sc * nseg, TX, sc % TX, nseg, 0, 1,
-                                       [] {});
-        else
-        for (int half = 1; half < nseg; half <<= 1) {
-            const int groups = (nseg + 2 * half - 1) / (2 * half);
-            for (int lane = 0; lane < lanes; lane++)
-                for (int g = lane; g < groups; g += lanes) {
-                    const int lo = g * 2 * half, mid = lo + half, hi = mid + half < nseg ? mid + half : nseg;
-                    if (mid < nseg)
-                        dolk::hull_merge<TIn>(sc >= TX ? F1 : F0, HM.data() + (size_t)sc * nseg, TX, sc % TX, lo,
-                                              mid, hi);
-                }
+        for (int col = 0; col < TX; col++) dolk::hull_build<TIn>(F0, F1, HM.data(), TX, nseg, n, col, seg);
+    for (int half = 1; half < nseg; half <<= 1)
+        for (int lo = 0; lo + half < nseg; lo += 2 * half) {
+            const int mid = lo + half, hi = mid + half < nseg ? mid + half : nseg;
+            for (int sc = 0; sc < 2 * TX; sc++)
+                dolk::hull_merge<TIn>(sc >= TX ? F1 : F0, HM.data() + (size_t)sc * nseg, TX, sc % TX, lo, mid, hi);
         }
     for (int seg = 0; seg < nseg; seg++)
         for (int col = 0; col < TX; col++)
-            for (int s = 0; s < (split ? 2 : 1); s++)
-                dolk::hull_query<TIn>(
-                    F0, F1, HM.data(), TX, nseg, n, col, seg,
-                    [&](int p, int, uint32_t b, bool nn) {
-                        best[(size_t)p * TX + col] = b;
-                        none[(size_t)p * TX + col] = nn ? 1 : 0;
-                    },
-                    split ? s : -1);
+            dolk::hull_query<TIn>(F0, F1, HM.data(), TX, nseg, n, col, seg, [&](int p, int, uint32_t b, bool nn) {
+                best[(size_t)p * TX + col] = b;
+                none[(size_t)p * TX + col] = nn ? 1 : 0;
+            });
 }
 
 // F0 / F1: split tiles of (32 * ceil(n / 32)) rows x TX columns, position 0 first
-extern "C" void hull_tile_u16(int n, int TX, const uint16_t* F0, const uint16_t* F1, uint32_t* best, uint8_t* none,
-                              int split, int lanes)
+extern "C" void hull_tile_u16(int n, int TX, const uint16_t* F0, const uint16_t* F1, uint32_t* best, uint8_t* none)
 {
-    run_tile<uint16_t>(n, TX, F0, F1, best, none, split, lanes);
+    run_tile<uint16_t>(n, TX, F0, F1, best, none);
 }
 
-extern "C" void hull_tile_u32(int n, int TX, const uint32_t* F0, const uint32_t* F1, uint32_t* best, uint8_t* none,
-                              int split, int lanes)
+extern "C" void hull_tile_u32(int n, int TX, const uint32_t* F0, const uint32_t* F1, uint32_t* best, uint8_t* none)
 {
-    run_tile<uint32_t>(n, TX, F0, F1, best, none, split, lanes);
+    run_tile<uint32_t>(n, TX, F0, F1, best, none);
 }

@@ -62,26 +62,29 @@ def brute(states, vals, dtype):
     return best, none
 
 
-def run_case(hull, states, vals, dtype, split=0, lanes=32):
+def run_case(hull, states, vals, dtype):
     F0, F1 = make_tile(states, vals, dtype)
     n, tx = states.shape
     rows = F0.shape[0]
     best = np.zeros((rows, tx), np.uint32)
     none = np.zeros((rows, tx), np.uint8)
     fn = hull.hull_tile_u16 if dtype == np.uint16 else hull.hull_tile_u32
-    fn(C.c_int(n), C.c_int(tx), _p(np.ascontiguousarray(F0)), _p(np.ascontiguousarray(F1)), _p(best), _p(none),
-       C.c_int(split), C.c_int(lanes))
+    fn(C.c_int(n), C.c_int(tx), _p(np.ascontiguousarray(F0)), _p(np.ascontiguousarray(F1)), _p(best), _p(none))
     want, want_none = brute(states, vals, dtype)
     np.testing.assert_array_equal(none[:n].astype(bool), want_none)
     np.testing.assert_array_equal(np.where(want_none, 0, best[:n]), np.where(want_none, 0, want))
 
 
-CASES = ["random", "sparse", "empty", "full", "constant", "runs", "single"]
+CASES = ["random", "sparse", "empty", "full", "constant", "runs", "single", "large"]
 
 
 def gen(kind, n, tx, dtype, rng):
     hi = 300 if dtype == np.uint16 else 90000
-    if kind == "random":
+    if kind == "large":        # own values near the largest a 16384-cell side gives
+        top = 16383 if dtype == np.uint16 else 2 * 16383 * 16383
+        st = (rng.random((n, tx)) < 0.3).astype(np.int64)
+        v = top - rng.integers(0, top // 50, (n, tx))
+    elif kind == "random":
         st = (rng.random((n, tx)) < 0.5).astype(np.int64)
         v = rng.integers(1, hi, (n, tx))
         v[rng.random((n, tx)) < 0.1] = 0
@@ -117,5 +120,3 @@ def test_hull_matches_brute_force(hull, dtype, kind, n):
     tx = 4
     st, v = gen(kind, n, tx, dtype, rng)
     run_case(hull, st, v, dtype)
-    run_case(hull, st, v, dtype, split=1, lanes=3)
-    run_case(hull, st, v, dtype, split=1, lanes=1)

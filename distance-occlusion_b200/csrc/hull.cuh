@@ -17,7 +17,8 @@
 // nearest for a state-s cell, the adjacent one is closer).
 //
 // Representation: per column and transform, a bitmask over positions (one
-// 32-bit word per 32-cell segment).  A (column, segment) unit builds its
+// 32-bit word per segment of SB = 32 cells, or 16 cells for 8-column tiles,
+// only the low SB bits used).  A (column, segment) unit builds its
 // segment's hull as a stack of set bits; segments merge pairwise in a tree
 // (the lower bridge of two x-separated hulls, walked from their facing ends,
 // clearing the vertices it passes); each unit then walks its cells left to
@@ -66,57 +67,63 @@ DOL_HD bool hull_keep(int xa, int ya, int xb, int yb, int xc, int yc)
     return (long long)(xb - xa) * (long long)(yc - ya) - (long long)(xc - xa) * (long long)(yb - ya) > 0;
 }
 
-// nearest vertex after v in words [.., hi) / before v in words [lo, ..); -1 if none
+// Positions map to hull words SB cells each (SB = 32, or 16 for 8-column
+// tiles so that every thread of the CTA holds a segment): word v / SB, bit
+// v % SB.  Nearest vertex after v in words [.., hi) / before v in words
+// [lo, ..); -1 if none.
+template <int SB>
 DOL_HD int hull_next(const uint32_t* W, int v, int hi)
 {
-    int wi = v >> 5;
-    uint32_t m = (v & 31) == 31 ? 0u : (W[wi] & (0xFFFFFFFEu << (v & 31)));
+    int wi = v / SB;
+    uint32_t m = W[wi] & ~((2u << (v % SB)) - 1u);
     while (!m) {
         if (++wi >= hi) return -1;
         m = W[wi];
     }
-    return (wi << 5) + ffs32(m);
+    return wi * SB + ffs32(m);
 }
 
+template <int SB>
 DOL_HD int hull_prev(const uint32_t* W, int v, int lo)
 {
-    int wi = v >> 5;
-    uint32_t m = W[wi] & ((1u << (v & 31)) - 1u);
+    int wi = v / SB;
+    uint32_t m = W[wi] & ((1u << (v % SB)) - 1u);
     while (!m) {
         if (--wi < lo) return -1;
         m = W[wi];
     }
-    return (wi << 5) + hibit32(m);
+    return wi * SB + hibit32(m);
 }
 
 // Segment hulls of both transforms for unit (col, seg) of a line of n cells,
 // written to HM[(s * TXv + col) * nseg + seg].
-template <typename TIn>
+template <typename TIn, int SB = 32>
 DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int nseg, int n, int col, int seg)
 {
-    const int p0 = seg << 5;
+    const int p0 = seg * SB;
     const uint32_t sent = sizeof(TIn) == 2 ? 0x7FFFu : 0x7FFFFFFFu;
     uint32_t S = 0, inf = 0;   // state bits; own value "none"
-    for (int i = 0; i < 32; i++) {
+    for (int i = 0; i < SB; i++) {
         // rotated by the segment: the units of a warp, in consecutive
         // segments, then read rows in different shared-memory banks
-        const int t = (i + seg) & 31, p = p0 + t;
+        const int t = (i + seg) & (SB - 1), p = p0 + t;
         const uint32_t r0 = F0[p * TXv + col], r1 = F1[p * TXv + col];
         S |= (uint32_t)(r1 != 0) << t;
         inf |= (uint32_t)((r0 | r1) == sent) << t;
     }
-    const uint32_t live = n - p0 >= 32 ? 0xFFFFFFFFu : ((1u << (n - p0)) - 1u);
+    const uint32_t full = SB == 32 ? 0xFFFFFFFFu : ((1u << SB) - 1u);
+    const uint32_t live = n - p0 >= SB ? full : ((1u << (n - p0)) - 1u);
     // the states just outside the segment (outside the line: neither)
-    const bool pv = p0 > 0, nx = p0 + 32 < n;
+    const bool pv = p0 > 0, nx = p0 + SB < n;
     const uint32_t s_prev = pv ? (uint32_t)(F1[(p0 - 1) * TXv + col] != 0) : 0u;
-    const uint32_t s_next = nx ? (uint32_t)(F1[(p0 + 32) * TXv + col] != 0) : 0u;
+    const uint32_t s_next = nx ? (uint32_t)(F1[(p0 + SB) * TXv + col] != 0) : 0u;
     for (int s = 0; s < 2; s++) {
         const TIn* Fs = s ? F1 : F0;
         const uint32_t own = (s ? S : ~S) & live;
         const uint32_t other = (s ? ~S : S) & live;
         const uint32_t own_prev = pv && (s ? s_prev : !s_prev) ? 1u : 0u;
         const uint32_t own_next = nx && (s ? s_next : !s_next) ? 1u : 0u;
-        const uint32_t near_own = (own << 1) | (own >> 1) | own_prev | (own_next << 31);
+        const uint32_t near_own = (own << 1) | (own >> 1) | own_prev | (own_next << (SB - 1));
         uint32_t cand = (own & ~inf) | (other & near_own);
         uint32_t M = 0;
         int xa = -1, xb = -1;
@@ -149,33 +156,33 @@ DOL_HD void hull_build(const TIn* F0, const TIn* F1, uint32_t* HM, int TXv, int 
 }
 
 // Merges the hulls of segments [lo, mid) and [mid, hi) of one (state, column).
-template <typename TIn>
+template <typename TIn, int SB = 32>
 DOL_HD void hull_merge(const TIn* Fs, uint32_t* W, int TXv, int col, int lo, int mid, int hi)
 {
     int a = -1, b = -1;
     for (int i = mid - 1; i >= lo && a < 0; i--)
-        if (W[i]) a = (i << 5) + hibit32(W[i]);
+        if (W[i]) a = i * SB + hibit32(W[i]);
     if (a < 0) return;
     for (int i = mid; i < hi && b < 0; i++)
-        if (W[i]) b = (i << 5) + ffs32(W[i]);
+        if (W[i]) b = i * SB + ffs32(W[i]);
     if (b < 0) return;
     int ya = hull_y<TIn>(Fs, a, TXv, col), yb = hull_y<TIn>(Fs, b, TXv, col);
     for (;;) {
-        const int ap = hull_prev(W, a, lo);
+        const int ap = hull_prev<SB>(W, a, lo);
         if (ap >= 0) {
             const int yp = hull_y<TIn>(Fs, ap, TXv, col);
             if (!hull_keep(ap, yp, a, ya, b, yb)) {
-                W[a >> 5] &= ~(1u << (a & 31));
+                W[a / SB] &= ~(1u << (a % SB));
                 a = ap;
                 ya = yp;
                 continue;
             }
         }
-        const int bn = hull_next(W, b, hi);
+        const int bn = hull_next<SB>(W, b, hi);
         if (bn >= 0) {
             const int yn = hull_y<TIn>(Fs, bn, TXv, col);
             if (!hull_keep(a, ya, b, yb, bn, yn)) {
-                W[b >> 5] &= ~(1u << (b & 31));
+                W[b / SB] &= ~(1u << (b % SB));
                 b = bn;
                 yb = yn;
                 continue;
@@ -195,7 +202,7 @@ DOL_HD uint32_t hull_at(const TIn* Fs, int v, int p, int TXv, int col)
 
 // The cells of unit (col, seg) against the merged hulls: emit(p, s, best,
 // none) per cell p < n, best = the transform's value (meaningless if none).
-template <typename TIn, class Emit>
+template <typename TIn, int SB = 32, class Emit>
 DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv, int nseg, int n, int col, int seg,
                        Emit&& emit)
 {
@@ -204,7 +211,7 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
     // right, so r stays valid until c moves, and the scan over empty hull
     // words to find it is done once per move, not once per cell
     int c0 = -2, c1 = -2, r0 = -2, r1 = -2;
-    const int p0 = seg << 5, p1 = n < p0 + 32 ? n : p0 + 32;
+    const int p0 = seg * SB, p1 = n < p0 + SB ? n : p0 + SB;
     for (int p = p0; p < p1; p++) {
         const int s = F1[p * TXv + col] != 0;
         const TIn* Fs = s ? F1 : F0;
@@ -213,14 +220,14 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
         if (c == -2) {   // first cell of this state in the unit: place the pointer
             // the first vertex at or after p, else the last one before it
             if (p == 0)
-                c = (W[0] & 1u) ? 0 : hull_next(W, 0, nseg);
+                c = (W[0] & 1u) ? 0 : hull_next<SB>(W, 0, nseg);
             else
-                c = hull_next(W, p - 1, nseg);
-            if (c < 0 && p > 0) c = hull_prev(W, p, 0);
+                c = hull_next<SB>(W, p - 1, nseg);
+            if (c < 0 && p > 0) c = hull_prev<SB>(W, p, 0);
             if (c >= 0) {
                 uint32_t cv = hull_at<TIn>(Fs, c, p, TXv, col);
                 for (;;) {   // the values along the hull are convex: walk down to the left
-                    const int l = hull_prev(W, c, 0);
+                    const int l = hull_prev<SB>(W, c, 0);
                     if (l < 0) break;
                     const uint32_t lv = hull_at<TIn>(Fs, l, p, TXv, col);
                     if (lv > cv) break;
@@ -233,13 +240,13 @@ DOL_HD void hull_query(const TIn* F0, const TIn* F1, const uint32_t* HM, int TXv
         uint32_t best = 0xFFFFFFFFu;
         if (c >= 0) {
             best = hull_at<TIn>(Fs, c, p, TXv, col);
-            if (r == -2) r = hull_next(W, c, nseg);
+            if (r == -2) r = hull_next<SB>(W, c, nseg);
             while (r >= 0) {   // and to the right, as p advances
                 const uint32_t rv = hull_at<TIn>(Fs, r, p, TXv, col);
                 if (rv > best) break;
                 c = r;
                 best = rv;
-                r = hull_next(W, c, nseg);
+                r = hull_next<SB>(W, c, nseg);
             }
         }
         if (s) {

@@ -436,12 +436,13 @@ __device__ __forceinline__ uint32_t far_side(uint32_t best, int q, int n, int k,
 }
 
 // the two split line arrays with their sentinel rows, then the envelope
-// path's hull words (two per column per 32-cell segment)
+// path's hull words (two per column per segment of 32 cells, 16 for 8-column tiles)
 template <typename TIn, int TX>
 static size_t tma_tile_bytes(int n)
 {
+    constexpr int SB = TX == 8 ? 16 : 32;
     return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn) +
-           2 * (size_t)TX * ((n + 31) / 32) * sizeof(uint32_t);
+           2 * (size_t)TX * ((n + SB - 1) / SB) * sizeof(uint32_t);
 }
 
 // One 32-bit word of a staged tile split by state: its cells (two uint16 or
@@ -466,7 +467,7 @@ __device__ __forceinline__ void split_word(uint32_t x, uint32_t vmask, uint32_t*
 template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
-                                                      int along_z, int form, int* err, int outer0, uint32_t hull_thr)
+                                                      int along_z, int form, int* err, int outer0, uint32_t hull_pct)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
@@ -516,19 +517,15 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     uint4* V1 = reinterpret_cast<uint4*>(F1);
     const uint32_t sw = sizeof(TIn) == 2 ? 0x7FFF7FFFu : 0x7FFFFFFFu;   // a word of sentinels / value bits
     const uint4 sent = make_uint4(sw, sw, sw, sw);
-    // while splitting, count the cells whose own value (their distance to the
-    // other state in the lower dimensions) exceeds the window threshold
-    // hull_thr, a cell with none counting 16 times (its walk would run to the
-    // line end): when they make up a quarter of the tile, it takes the
-    // envelope path.  Dense fields have few such cells, sparse ones mostly.
-    const uint32_t thr = sizeof(TIn) == 2 ? (hull_thr > 0x7FFEu ? 0x7FFEu : hull_thr) * 0x00010001u
-                                          : (hull_thr >= 46341u ? 0x7FFFFFFEu : hull_thr * hull_thr);
+    // while splitting, count the cells with no cell of the other state on
+    // their lower-dimension lines ("none"): their windowed walk runs to the
+    // line end.  When they make up hull_pct percent of the tile (sparse or
+    // empty volumes), the tile takes the envelope path.
     uint32_t score = 0;
     auto weigh = [&](uint32_t x) -> uint32_t {
         const uint32_t v = x & sw;
-        if (sizeof(TIn) == 2)
-            return (__popc(__vcmpgtu2(v, thr)) + 15 * __popc(__vcmpeq2(v, sw))) >> 4;
-        return (v > thr ? 1u : 0u) + (v == sw ? 15u : 0u);
+        if (sizeof(TIn) == 2) return __popc(__vcmpeq2(v, sw)) >> 4;
+        return v == sw ? 1u : 0u;
     };
     for (int i = threadIdx.x; i < n * kVecRow; i += blockDim.x) {
         const uint4 x = V0[i];
@@ -553,16 +550,17 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     if ((threadIdx.x & 31) == 0 && score) atomicAdd(&s_score, score);
     __syncthreads();
     const long long tile_cells = (long long)n * min(TX, w - x0);
-    const bool use_hull = hull_thr == 0u || (hull_thr != 0xFFFFFFFFu && 4LL * s_score > tile_cells);
+    const bool use_hull = hull_pct <= 100u && 100LL * s_score >= (long long)hull_pct * tile_cells;
 
     if (use_hull) {
         // envelope path: units (column, 32-cell segment); hull words after the tile
-        const int nseg = (n + 31) >> 5;
+        constexpr int SB = TX == 8 ? 16 : 32;   // cells per segment: TX * (1024 / SB) = 512 units for 1024 cells
+        const int nseg = (n + SB - 1) / SB;
         uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
         const int units = TX * nseg;
         for (int u = threadIdx.x; u < units; u += blockDim.x) {
             const int col = u % TX, seg = u / TX;
-            if (x0 + col < w) hull_build<TIn>(F0, F1, HM, TX, nseg, n, col, seg);
+            if (x0 + col < w) hull_build<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg);
         }
         __syncthreads();
         for (int half = 1; half < nseg; half <<= 1) {
@@ -572,7 +570,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
                 const int col = sc % TX, s = sc / TX;
                 const int lo = g * 2 * half, mid = lo + half, hi = min(mid + half, nseg);
                 if (mid < nseg && x0 + col < w)
-                    hull_merge<TIn>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
+                    hull_merge<TIn, SB>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
             }
             __syncthreads();
         }
@@ -583,7 +581,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
             if (x >= w) continue;
             const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
                                               : (long long)outer * outer_stride + x;
-            hull_query<TIn>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
+            hull_query<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
                 put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best, none || best >= kNoneH,
                                        form);
             });
@@ -726,19 +724,18 @@ static bool blocked_layout_ok(const uint16_t* vx, const uint32_t* ey, int w, int
     return line_map<uint16_t, 16>(&m, vx, w, h, d, 0, 1) && line_map<uint32_t, 8>(&m, ey, w, h, d, 1, 2);
 }
 
-// Window threshold of the line passes: a tile where a quarter of the cells
-// (a cell with no other-state cell on its lower-dimension lines counting 16)
-// lie farther than this from the other state in the lower dimensions takes
-// the envelope path.  The tuned value (DOL_TUNE_EDT_HULL, by line length): 1 =
-// windowed search only, 2 = envelope only, >= 3 = that distance; 0 = 64
-// (1 % of the cells of the 50 % noise volume lie farther, every cell of a
-// volume of scattered points does).
-static uint32_t edt_hull_threshold(int n)
+// Share of "none" cells (percent) at which a line-pass tile takes the
+// envelope path; above 100: never.  The tuned value (DOL_TUNE_EDT_HULL, by
+// line length): 1 = windowed search only, 2 = envelope only, 3..100 = that
+// percentage; 0 = 50 (the tiles of sparse and empty volumes; dense fields,
+// and fields whose far cells still see a candidate, keep the windowed search,
+// which is faster there).
+static uint32_t edt_hull_share(int n)
 {
     const int v = tune_get(kTuneEdtHull, n);
     if (v == 1) return 0xFFFFFFFFu;
     if (v == 2) return 0u;
-    return v >= 3 ? (uint32_t)v : 64u;
+    return v >= 3 && v <= 100 ? (uint32_t)v : 50u;
 }
 
 // Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
@@ -760,7 +757,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
     const int tv = tune_get(kTuneEdt, w);
     const int threads = tv == 256 ? 256 : 512;
-    const uint32_t hthr = edt_hull_threshold(n);
+    const uint32_t hthr = edt_hull_share(n);
     CUtensorMap map;
     if (mode == 1) {
         if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) return;   // blocked_layout_ok encoded it already

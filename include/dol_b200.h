@@ -331,9 +331,10 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_DANIELSSON_ROWS 8 /* Danielsson block schedule: rows per block (1..4096);
                                       65536 = the serial single-CTA engine */
 #define DOL_TUNE_DANIELSSON_SLICES 9 /* Danielsson block schedule: slices per block (3D) */
-#define DOL_TUNE_EDT_HULL     10   /* EDT line passes, by line length: a tile whose cells lie farther than this
-                                      from the other state along the lower dimensions takes the lower-envelope
-                                      path instead of the windowed search; 1 = window only, 2 = envelope only */
+#define DOL_TUNE_EDT_HULL     10   /* EDT line passes, by line length: the percentage of a tile's cells with no
+                                      other-state cell on their lower-dimension lines at which the tile takes the
+                                      lower-envelope path instead of the windowed search (0 = 50);
+                                      1 = windowed search only, 2 = envelope only */
 DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream);
 DOL_API int        dol_tune_get(int kind, int w);
 DOL_API void       dol_tune_set(int kind, int w, int value);

@@ -62,14 +62,15 @@ def brute(states, vals, dtype):
     return best, none
 
 
-def run_case(hull, states, vals, dtype):
+def run_case(hull, states, vals, dtype, sb=32):
     F0, F1 = make_tile(states, vals, dtype)
     n, tx = states.shape
     rows = F0.shape[0]
     best = np.zeros((rows, tx), np.uint32)
     none = np.zeros((rows, tx), np.uint8)
     fn = hull.hull_tile_u16 if dtype == np.uint16 else hull.hull_tile_u32
-    fn(C.c_int(n), C.c_int(tx), _p(np.ascontiguousarray(F0)), _p(np.ascontiguousarray(F1)), _p(best), _p(none))
+    fn(C.c_int(n), C.c_int(tx), _p(np.ascontiguousarray(F0)), _p(np.ascontiguousarray(F1)), _p(best), _p(none),
+       C.c_int(sb))
     want, want_none = brute(states, vals, dtype)
     np.testing.assert_array_equal(none[:n].astype(bool), want_none)
     np.testing.assert_array_equal(np.where(want_none, 0, best[:n]), np.where(want_none, 0, want))
@@ -120,3 +121,4 @@ def test_hull_matches_brute_force(hull, dtype, kind, n):
     tx = 4
     st, v = gen(kind, n, tx, dtype, rng)
     run_case(hull, st, v, dtype)
+    run_case(hull, st, v, dtype, sb=16)

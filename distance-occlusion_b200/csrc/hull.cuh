@@ -17,8 +17,8 @@
 // nearest for a state-s cell, the adjacent one is closer).
 //
 // Representation: per column and transform, a bitmask over positions (one
-// 32-bit word per segment of SB = 32 cells, or 16 cells for 8-column tiles,
-// only the low SB bits used).  A (column, segment) unit builds its
+// 32-bit word per segment of SB cells, only the low SB bits used; the kernel
+// uses SB = 32, the CPU tests 16 as well).  A (column, segment) unit builds its
 // segment's hull as a stack of set bits; segments merge pairwise in a tree
 // (the lower bridge of two x-separated hulls, walked from their facing ends,
 // clearing the vertices it passes); each unit then walks its cells left to
@@ -67,9 +67,7 @@ DOL_HD bool hull_keep(int xa, int ya, int xb, int yb, int xc, int yc)
     return (long long)(xb - xa) * (long long)(yc - ya) - (long long)(xc - xa) * (long long)(yb - ya) > 0;
 }
 
-// Positions map to hull words SB cells each (SB = 32, or 16 for 8-column
-// tiles so that every thread of the CTA holds a segment): word v / SB, bit
-// v % SB.  Nearest vertex after v in words [.., hi) / before v in words
+// Positions map to hull words SB cells each: word v / SB, bit v % SB.  Nearest vertex after v in words [.., hi) / before v in words
 // [lo, ..); -1 if none.
 template <int SB>
 DOL_HD int hull_next(const uint32_t* W, int v, int hi)

@@ -436,11 +436,11 @@ __device__ __forceinline__ uint32_t far_side(uint32_t best, int q, int n, int k,
 }
 
 // the two split line arrays with their sentinel rows, then the envelope
-// path's hull words (two per column per segment of 32 cells, 16 for 8-column tiles)
+// path's hull words (two per column per 32-cell segment)
 template <typename TIn, int TX>
 static size_t tma_tile_bytes(int n)
 {
-    constexpr int SB = TX == 8 ? 16 : 32;
+    constexpr int SB = 32;
     return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn) +
            2 * (size_t)TX * ((n + SB - 1) / SB) * sizeof(uint32_t);
 }
@@ -554,7 +554,9 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
 
     if (use_hull) {
         // envelope path: units (column, 32-cell segment); hull words after the tile
-        constexpr int SB = TX == 8 ? 16 : 32;   // cells per segment: TX * (1024 / SB) = 512 units for 1024 cells
+        // cells per segment (16-cell segments, which keep every thread of an
+        // 8-column tile busy, measured slower: more words to scan and merge)
+        constexpr int SB = 32;
         const int nseg = (n + SB - 1) / SB;
         uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
         const int units = TX * nseg;

@@ -323,8 +323,10 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
     """Secondary measurements on the other workloads: the 2D default
     (1024^2, 100 points, seed 1, unsigned Danielsson), the 256^3 signed volume
     (32 boxes + 32 spheres, sizes 4-40, seed 7) with every method, the batch
-    of 4096 uneven masks + 64 volumes (batched launch vs per-item loop), and
-    Danielsson on the 1024^3 noise volume.  GPU times are CUDA events on
+    of 4096 uneven masks + 64 volumes (batched launch vs per-item loop),
+    Danielsson on the 1024^3 noise volume, the mask EDT where the other state
+    is far (a sparse 2D image, 1024^3 volumes of 2000 points and of none), and
+    the occlusion sweeps and mesh voxeliser.  GPU times are CUDA events on
     device-resident data; CPU times are the reference library (oracle/_ref),
     one thread, on the same inputs."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -355,6 +357,8 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
         _config3(dol, torch, res, L, sp)
     if want("c7"):
         _config_sparse(dol, torch, O, ref, res, L, sp, big)
+    if want("c8"):
+        _config_occlusion_voxel(dol, torch, O, ref, res)
     if only is not None and "c6" in only:
         _sweep_variants(dol, torch, res, L, sp, big)
     return res
@@ -657,6 +661,48 @@ def _config_sparse(dol, torch, O, ref, res, L, sp, big=True):
     res["edt_sparse"] = out
 
 
+def _config_occlusion_voxel(dol, torch, O, ref, res):
+    """The occlusion sweeps (2D default image; 256^3 value noise, lattice 16,
+    seed 3) and the mesh voxeliser (the reference's sample mesh at 256^3), GPU
+    against the reference's CPU code (one thread) on the same inputs."""
+    import ctypes as C
+    out = {}
+    for dims in ((1024, 1024), (256, 256, 256)):
+        if len(dims) == 2:
+            m = dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
+        else:
+            m = np.zeros(dol.mask_words(*dims), np.uint32)
+            dol.lib().dol_gen_value_noise_3d_host(*dims, SPACING, C.c_uint32(SEED), m.ctypes.data_as(C.c_void_p))
+        md = torch.from_numpy(m.view(np.int32)).cuda()
+        dw = dol.init_dirw(md, dims)
+        run = lambda: dol.occlusion_sweep(dol.init_dirw(md, dims, out=dw), dims)
+        run()
+        torch.cuda.synchronize()
+        key = "x".join(map(str, dims))
+        out[f"occlusion_{key}_ms"] = min(_ev_ms(torch, run, 1) for _ in range(3))
+        if ref is not None:
+            t0 = time.perf_counter()
+            O.occlusion_sweep(O.init_dirw(m, dims, use_ref=True), dims, use_ref=True)
+            out[f"cpu_ref_occlusion_{key}_ms"] = (time.perf_counter() - t0) * 1e3
+    tri = os.path.join(ROOT, "oracle", "_ref", "plant2.tri")
+    if os.path.exists(tri):
+        idx, v, bb = O.load_tri(tri)
+        it, vt = torch.from_numpy(idx).cuda(), torch.from_numpy(v).cuda()
+        n = 256
+        mv = torch.zeros(dol.mask_words(n, n, n), dtype=torch.int32, device="cuda")
+        run = lambda: dol.voxelize(it, vt, bb, (n, n, n), mask=mv)
+        run()
+        torch.cuda.synchronize()
+        out["voxelize_plant2_256_ms"] = min(_ev_ms(torch, run, 1) for _ in range(3))
+        out["voxelize_triangles"] = int(idx.shape[0])
+        if ref is not None:
+            t0 = time.perf_counter()
+            O.voxelize(idx, v, bb, (n, n, n), use_ref=True)
+            out["cpu_ref_voxelize_plant2_256_ms"] = (time.perf_counter() - t0) * 1e3
+    res["occlusion_voxel"] = {"workload": "occlusion sweeps: 1024^2 (100 points, seed 1) and 256^3 value noise; "
+                                          "voxeliser: the reference's sample mesh (plant2) at 256^3", **out}
+
+
 def _batch_item_type():
     class Item(C.Structure):
         _fields_ = [("w", C.c_int), ("h", C.c_int), ("d", C.c_int), ("reserved", C.c_int),
@@ -935,7 +981,7 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration measurements")
     ap.add_argument("--no-big", action="store_true", help="skip Danielsson on the 1024^3 volume")
     ap.add_argument("--only", default=None,
-                    help="comma list of c1..c7: run only these per-configuration measurements (no headline)")
+                    help="comma list of c1..c8: run only these per-configuration measurements (no headline)")
     ap.add_argument("--case", default=None, choices=CASES, help="run one kernel family's small workload (profiling)")
     ap.add_argument("--danielsson", default=None, metavar="WxHxD",
                     help="only time signed Danielsson on a WxHxD value-noise volume (twice; for profiling)")

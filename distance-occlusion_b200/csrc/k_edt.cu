@@ -464,6 +464,50 @@ __device__ __forceinline__ void split_word(uint32_t x, uint32_t vmask, uint32_t*
 // O(n) per cell.  Tiles holding such values take the lower-envelope path,
 // O(n) per line whatever the data.
 
+// The envelope path of one staged tile (hull.cuh), out of line so that the
+// windowed search's code is laid out and register-allocated as if it were
+// alone in the kernel (inlined, the dense tiles' passes measured 1-3 % slower).
+template <typename TIn, bool kFinal, int TX, int kMode>
+__device__ __noinline__ void edt_tile_envelope(const TIn* F0, TIn* F1, int rows, int n, int w, int x0, int outer,
+                                               void* out, long long stride, long long outer_stride, int form)
+{
+    // envelope path: units (column, 32-cell segment); hull words after the tile
+    // cells per segment (16-cell segments, which keep every thread of an
+    // 8-column tile busy, measured slower: more words to scan and merge)
+    constexpr int SB = 32;
+    const int nseg = (n + SB - 1) / SB;
+    uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
+    const int units = TX * nseg;
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int col = u % TX, seg = u / TX;
+        if (x0 + col < w) hull_build<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg);
+    }
+    __syncthreads();
+    for (int half = 1; half < nseg; half <<= 1) {
+        const int groups = (nseg + 2 * half - 1) / (2 * half);
+        for (int j = threadIdx.x; j < 2 * TX * groups; j += blockDim.x) {
+            const int g = j % groups, sc = j / groups;   // sc = s * TX + col
+            const int col = sc % TX, s = sc / TX;
+            const int lo = g * 2 * half, mid = lo + half, hi = min(mid + half, nseg);
+            if (mid < nseg && x0 + col < w)
+                hull_merge<TIn, SB>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
+        }
+        __syncthreads();
+    }
+    const uint32_t kNoneH = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int col = u % TX, seg = u / TX;
+        const int x = x0 + col;
+        if (x >= w) continue;
+        const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
+                                          : (long long)outer * outer_stride + x;
+        hull_query<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
+            put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best, none || best >= kNoneH,
+                                   form);
+        });
+    }
+}
+
 template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
@@ -555,41 +599,7 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     const bool use_hull = hull_pct <= 100u && 100LL * s_score >= (long long)hull_pct * sampled;
 
     if (use_hull) {
-        // envelope path: units (column, 32-cell segment); hull words after the tile
-        // cells per segment (16-cell segments, which keep every thread of an
-        // 8-column tile busy, measured slower: more words to scan and merge)
-        constexpr int SB = 32;
-        const int nseg = (n + SB - 1) / SB;
-        uint32_t* HM = reinterpret_cast<uint32_t*>(F1 + (rows + 2 * kPadRows) * TX - kPadRows * TX);
-        const int units = TX * nseg;
-        for (int u = threadIdx.x; u < units; u += blockDim.x) {
-            const int col = u % TX, seg = u / TX;
-            if (x0 + col < w) hull_build<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg);
-        }
-        __syncthreads();
-        for (int half = 1; half < nseg; half <<= 1) {
-            const int groups = (nseg + 2 * half - 1) / (2 * half);
-            for (int j = threadIdx.x; j < 2 * TX * groups; j += blockDim.x) {
-                const int g = j % groups, sc = j / groups;   // sc = s * TX + col
-                const int col = sc % TX, s = sc / TX;
-                const int lo = g * 2 * half, mid = lo + half, hi = min(mid + half, nseg);
-                if (mid < nseg && x0 + col < w)
-                    hull_merge<TIn, SB>(s ? F1 : F0, HM + (size_t)sc * nseg, TX, col, lo, mid, hi);
-            }
-            __syncthreads();
-        }
-        const uint32_t kNoneH = sizeof(TIn) == 2 ? kInf16 * kInf16 : kInf32;
-        for (int u = threadIdx.x; u < units; u += blockDim.x) {
-            const int col = u % TX, seg = u / TX;
-            const int x = x0 + col;
-            if (x >= w) continue;
-            const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
-                                              : (long long)outer * outer_stride + x;
-            hull_query<TIn, SB>(F0, F1, HM, TX, nseg, n, col, seg, [&](int p, int s, uint32_t best, bool none) {
-                put_walk_value<kFinal>(out, base + (long long)p * stride, (uint32_t)s, best, none || best >= kNoneH,
-                                       form);
-            });
-        }
+        edt_tile_envelope<TIn, kFinal, TX, kMode>(F0, F1, rows, n, w, x0, outer, out, stride, outer_stride, form);
         return;
     }
 

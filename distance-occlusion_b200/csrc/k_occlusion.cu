@@ -22,7 +22,8 @@
 // owns C adjacent columns and walks the (slice, row) items in order, skewed
 // one step behind thread t-1, whose last column it takes from shared memory
 // (double-buffered by step parity); "up" stays in registers and "back" is
-// the thread's own output of h items before.
+// the thread's own output of h items before.  Rows of up to 1024 cells (one
+// column per thread) prefetch each item's loads a few steps ahead.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -131,6 +132,89 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep(float* __restrict__ ou
     }
 }
 
+// The same sweep for rows of up to 1024 cells, one column per thread, with
+// every global value an item needs loaded kP steps before its turn (the loop
+// is unrolled by kP, so the ring of loads stays in registers): a step then
+// waits on the barrier and the float chain, not on memory.  "back" (this
+// thread's own output h items earlier) is prefetched only when h > kP, after
+// it was written.
+template <int DIM, bool IO>
+__global__ void __launch_bounds__(1024) k_occlusion_sweep1(float* __restrict__ outp, const float* __restrict__ inp,
+                                                           int w, int h, int d)
+{
+    constexpr int kP = 4;
+    __shared__ float edge[2][1024];
+    const int sweep = blockIdx.x;
+    const int sx = sweep & 1, sy = (sweep >> 1) & 1, sz = (sweep >> 2) & 1;
+    const int dx = 1 - 2 * sx, dy = 1 - 2 * sy, dz = 1 - 2 * sz;
+    const long long wh = (long long)w * h;
+    const long long n = wh * d;
+    float* out = outp + sweep * n;
+    const float* in = IO ? inp + sweep * n : nullptr;
+    const int t = threadIdx.x;
+    const bool has = t < w;
+    const int x = sx ? w - 1 - t : t;
+    const long long Q = (long long)d * h;
+    const long long S = Q + w - 1;   // steps
+    const bool pre_back = DIM == 3 && h > kP;
+    float own[kP], bk[kP], il[kP], iu[kP], ib[kP];
+    auto cell = [&](long long q, int& jj, int& kk) -> long long {
+        kk = (int)(q / h);
+        jj = (int)(q - (long long)kk * h);
+        const int y = sy ? h - 1 - jj : jj, z = sz ? d - 1 - kk : kk;
+        return ((long long)z * h + y) * w + x;
+    };
+    auto fetch = [&](long long q, int slot) {
+        if (!has || q < 0 || q >= Q) return;
+        int jj, kk;
+        const long long c = cell(q, jj, kk);
+        own[slot] = out[c];
+        if (pre_back) bk[slot] = kk ? out[c - dz * wh] : 0.0f;
+        if (IO) {
+            il[slot] = t ? in[c - dx] : 0.0f;
+            iu[slot] = jj ? in[c - (long long)dy * w] : 0.0f;
+            ib[slot] = kk ? in[c - dz * wh] : 0.0f;
+        }
+    };
+#pragma unroll
+    for (int u = 0; u < kP; u++) fetch(u - t, u);
+    float up = 0.0f;
+    for (long long s0 = 0; s0 < S; s0 += kP) {
+#pragma unroll
+        for (int u = 0; u < kP; u++) {
+            const long long s = s0 + u;
+            if (s < S) {   // uniform: every thread runs the same steps
+                const long long q = s - t;
+                float last = 0.0f;
+                if (has && q >= 0 && q < Q) {
+                    int jj, kk;
+                    const long long c = cell(q, jj, kk);
+                    const float left = t ? edge[(s - 1) & 1][t - 1] : 0.0f;
+                    const float upv = jj ? up : 0.0f;
+                    float back = 0.0f;
+                    if (DIM == 3 && kk) back = pre_back ? bk[u] : out[c - dz * wh];
+                    float v;
+                    if (t == 0 && jj == 0 && kk == 0) {
+                        v = own[u];   // the starting corner keeps its value
+                    } else if (IO) {
+                        v = oct_combine_io(left, upv, back, il[u], iu[u], ib[u]);
+                        out[c] = v;
+                    } else {
+                        const float qv = DIM == 2 ? quad_combine(left, upv) : oct_combine(left, upv, back);
+                        v = occ_update(own[u], qv);
+                        out[c] = v;
+                    }
+                    up = v;
+                    last = v;
+                }
+                edge[s & 1][t] = last;
+                fetch(q + kP, u);
+                __syncthreads();
+            }
+        }
+    }
+}
+
 void launch_init_dirw(int dim, const uint32_t* mask, float* dirw, int w, int h, int d, cudaStream_t st)
 {
     const long long rows = (long long)h * (dim == 3 ? d : 1);
@@ -150,6 +234,15 @@ void launch_occlusion_sweep(int dim, float* dirw, const float* in, int w, int h,
     const int planes = dim == 3 ? 8 : 4;
     const int dd = dim == 3 ? d : 1;
     ProfScope ps(in ? "occlusion_sweep_io" : "occlusion_sweep", st);
+    if (C == 1) {
+        if (dim == 2)
+            k_occlusion_sweep1<2, false><<<planes, T, 0, st>>>(dirw, in, w, h, 1);
+        else if (!in)
+            k_occlusion_sweep1<3, false><<<planes, T, 0, st>>>(dirw, in, w, h, dd);
+        else
+            k_occlusion_sweep1<3, true><<<planes, T, 0, st>>>(dirw, in, w, h, dd);
+        return;
+    }
 #define DOL_OCC_CASE(DIMV, IOV, CV) \
     k_occlusion_sweep<DIMV, IOV, CV><<<planes, T, 0, st>>>(dirw, in, w, h, dd)
     if (dim == 2) {

@@ -578,10 +578,12 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         split_word<TIn>(x.w, sw, &a.w, &b.w);
         V0[i] = a;
         V1[i] = b;
-        if (sizeof(TIn) == 2)
-            score += __vcmpeq2(x.x & sw, sw) & 0x00010001u;   // one per "none" half, summed per half
-        else
-            score += (x.x & sw) == sw;
+        if (hull_pct <= 100u) {   // uniform; skipped when the envelope path is off
+            if (sizeof(TIn) == 2)
+                score += __vcmpeq2(x.x & sw, sw) & 0x00010001u;   // one per "none" half, summed per half
+            else
+                score += (x.x & sw) == sw;
+        }
     }
     for (int i = n * kVecRow + threadIdx.x; i < (rows + kPadRows) * kVecRow; i += blockDim.x) {
         V0[i] = sent;
@@ -777,6 +779,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) return;   // blocked_layout_ok encoded it already
         auto kern = k_edt_line_tma<TIn, kFinal, TX, 1>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         dim3 grid((w + TX - 1) / TX, (unsigned)outer);
         kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0, hthr);
         return;
@@ -790,6 +793,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         }
         auto kern = k_edt_line_tma<TIn, kFinal, 8, 2>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         const unsigned blocks = (unsigned)(outer * (w / 8));
         kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0, hthr);
         return;
@@ -798,6 +802,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         if (line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) {
             auto kern = k_edt_line_tma<TIn, kFinal, TX, 0>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
             kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0,
                                                     hthr);

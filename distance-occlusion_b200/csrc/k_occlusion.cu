@@ -92,11 +92,16 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep(float* __restrict__ ou
 #pragma unroll
     for (int u = 0; u < C; u++) up[u] = 0.0f;
     const long long Q = (long long)d * h;
+    int cj = 0, ck = 0;   // (row, slice) of the next item, kept as running counters
     for (long long s = 0; s < Q + T - 1; s++) {
         const long long q = s - t;
         float last = 0.0f;
         if (q >= 0 && q < Q && ncol > 0) {
-            const int kk = (int)(q / h), jj = (int)(q - (long long)kk * h);
+            const int kk = ck, jj = cj;
+            if (++cj == h) {
+                cj = 0;
+                ck++;
+            }
             const int y = sy ? h - 1 - jj : jj, z = sz ? d - 1 - kk : kk;
             const long long rowbase = ((long long)z * h + y) * w;
             float left = ii0 > 0 ? edge[(s - 1) & 1][t - 1] : 0.0f;
@@ -158,16 +163,12 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep1(float* __restrict__ o
     const long long S = Q + w - 1;   // steps
     const bool pre_back = DIM == 3 && h > kP;
     float own[kP], bk[kP], il[kP], iu[kP], ib[kP];
-    auto cell = [&](long long q, int& jj, int& kk) -> long long {
-        kk = (int)(q / h);
-        jj = (int)(q - (long long)kk * h);
+    auto cell = [&](int jj, int kk) -> long long {
         const int y = sy ? h - 1 - jj : jj, z = sz ? d - 1 - kk : kk;
         return ((long long)z * h + y) * w + x;
     };
-    auto fetch = [&](long long q, int slot) {
-        if (!has || q < 0 || q >= Q) return;
-        int jj, kk;
-        const long long c = cell(q, jj, kk);
+    auto fetch = [&](int jj, int kk, int slot) {
+        const long long c = cell(jj, kk);
         own[slot] = out[c];
         if (pre_back) bk[slot] = kk ? out[c - dz * wh] : 0.0f;
         if (IO) {
@@ -176,8 +177,19 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep1(float* __restrict__ o
             ib[slot] = kk ? in[c - dz * wh] : 0.0f;
         }
     };
+    // items are (row jj, slice kk) in order; step s processes item s - t and
+    // fetches item s - t + kP into the slot of step s % kP.  Both walk with
+    // running counters (a 64-bit division per step cost more than the sweep).
+    long long f = kP - t;   // the next item to fetch
+    int fj = 0, fk = 0;
+    if (f > 0) {
+        fk = (int)(f / h);
+        fj = (int)(f - (long long)fk * h);
+    }
 #pragma unroll
-    for (int u = 0; u < kP; u++) fetch(u - t, u);
+    for (int u = 0; u < kP; u++)   // items u - t: the first steps' slots
+        if (has && u - t >= 0 && u - t < Q) fetch((u - t) % h, (u - t) / h, u);
+    int cj = 0, ck = 0;   // the next item to process
     float up = 0.0f;
     for (long long s0 = 0; s0 < S; s0 += kP) {
 #pragma unroll
@@ -187,8 +199,8 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep1(float* __restrict__ o
                 const long long q = s - t;
                 float last = 0.0f;
                 if (has && q >= 0 && q < Q) {
-                    int jj, kk;
-                    const long long c = cell(q, jj, kk);
+                    const int jj = cj, kk = ck;
+                    const long long c = cell(jj, kk);
                     const float left = t ? edge[(s - 1) & 1][t - 1] : 0.0f;
                     const float upv = jj ? up : 0.0f;
                     float back = 0.0f;
@@ -206,9 +218,20 @@ __global__ void __launch_bounds__(1024) k_occlusion_sweep1(float* __restrict__ o
                     }
                     up = v;
                     last = v;
+                    if (++cj == h) {
+                        cj = 0;
+                        ck++;
+                    }
                 }
                 edge[s & 1][t] = last;
-                fetch(q + kP, u);
+                if (has && f >= 0 && f < Q) {
+                    fetch(fj, fk, u);
+                    if (++fj == h) {
+                        fj = 0;
+                        fk++;
+                    }
+                }
+                f++;
                 __syncthreads();
             }
         }

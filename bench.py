@@ -923,8 +923,8 @@ def run_case(name, reps=2):
         def fn():
             f.copy_(f0)
             dol.chamfer(f, dims)
-    elif name in ("occlusion_1024", "occlusion_128"):
-        n = int(name.split("_")[1])
+    elif name.startswith("occlusion_"):           # occlusion_1024 (2D), occlusion_128 / _256, occlusion_io_256
+        n = int(name.split("_")[-1])
         if n == 1024:
             dims = (1024, 1024)
             md = torch.from_numpy(dol.add_points(np.zeros(dol.mask_words(*dims), np.uint32), dims, 100, 1)
@@ -932,7 +932,11 @@ def run_case(name, reps=2):
         else:
             dims, md = _case_inputs(dol, torch, L, "noise", n)
         dw = dol.init_dirw(md, dims)
-        fn = lambda: dol.occlusion_sweep(dol.init_dirw(md, dims, out=dw), dims)
+        if "_io_" in name:
+            dout = dw.clone()
+            fn = lambda: dol.occlusion_sweep_io(dw, dout, dims)
+        else:
+            fn = lambda: dol.occlusion_sweep(dol.init_dirw(md, dims, out=dw), dims)
     elif name.startswith("voxel_"):                # voxel_256: the reference's sample mesh
         import oracle as O
         n = int(name.split("_")[1])
@@ -962,7 +966,8 @@ def run_case(name, reps=2):
 
 
 CASES = ["edt_noise_512", "edt_points_512", "edt_shapes_256", "border_256", "danielsson_256", "fastsweep_256",
-         "jumpflood_256", "dist_256", "chamfer_1024", "occlusion_1024", "occlusion_128", "voxel_256", "batch",
+         "jumpflood_256", "dist_256", "chamfer_1024", "occlusion_1024", "occlusion_128", "occlusion_256",
+         "occlusion_io_256", "voxel_256", "batch",
          "sites_512"]
 
 

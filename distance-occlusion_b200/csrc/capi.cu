@@ -624,13 +624,9 @@ dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* deltas, 
 
 // ---- occlusion ----------------------------------------------------------------------------------
 
-constexpr int kMaxOcclusionWidth = 4096;
-
 static dol_status occ_checks(int w, int h, int d)
 {
     DOL_TRY(check_dims(w, h, d));
-    if (w > kMaxOcclusionWidth)
-        return fail(DOL_ERR_UNSUPPORTED, "occlusion rows are limited to %d cells (got %d)", kMaxOcclusionWidth, w);
     if ((long long)d * h > (1LL << 40) / 8) return fail(DOL_ERR_INVALID_ARG, "volume too large");
     return DOL_OK;
 }

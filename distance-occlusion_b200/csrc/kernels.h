@@ -41,6 +41,7 @@ enum TuneKind {
     kTuneDanRows,
     kTuneDanSlices,
     kTuneEdtHull,
+    kTuneOcc,
     kTuneKinds
 };
 int tune_get(int kind, int w);
@@ -126,8 +127,14 @@ template <typename T>
 void launch_init_distances_int(const uint32_t* mask, T* dist, int w, long long rows, T max_d, cudaStream_t st);
 
 // k_occlusion.cu -- direction-weight planes (4 in 2D, 8 in 3D) and the
-// occlusion sweeps; in != nullptr selects the 3D in/out form (rows up to 4096)
+// occlusion sweeps; in != nullptr selects the 3D in/out form
 void launch_init_dirw(int dim, const uint32_t* mask, float* dirw, int w, int h, int d, cudaStream_t st);
+// engines (kTuneOcc): 0 = the block wavefront (2D tiles of 32 x 32, 3D blocks
+// of 32 x 16 columns x kOccSlicesPerBlock slices, 64 from 256 slices on),
+// 1 = one CTA per plane (rows up to kOccPlaneMaxWidth), 2..999 = 3D blocks of
+// that many slices, plus 1000 = blocks of 32 x 32 columns
+constexpr int kOccSlicesPerBlock = 32;
+constexpr int kOccPlaneMaxWidth = 4096;
 void launch_occlusion_sweep(int dim, float* dirw, const float* in, int w, int h, int d, cudaStream_t st);
 
 // k_voxel.cu -- triangles to bitmask (ORed into mask); bbox: min xyz, max xyz (host)

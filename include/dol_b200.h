@@ -211,7 +211,8 @@ DOL_API dol_status dol_deltas_to_dist_3d(int w, int h, int d, const dol_delta3* 
    OcclusionSweep (DistanceOcclusionLib.cpp:1173-1209, :2745-2769), in place;
    the 3D in/out form (:2771-2784) writes the occlusion caused by `in` to `out`
    (out's starting-corner cell of each plane is left as it was).  Bit-exact:
-   the reference's float operations in its order.  Rows up to 4096 cells. */
+   the reference's float operations in its order.  Any shape whose planes fit
+   the device. */
 DOL_API dol_status dol_init_dirw_2d(int w, int h, const uint32_t* mask, float* dirW, void* stream);
 DOL_API dol_status dol_init_dirw_3d(int w, int h, int d, const uint32_t* mask, float* dirW, void* stream);
 DOL_API dol_status dol_occlusion_sweep_2d(int w, int h, float* dirW, void* stream);
@@ -335,6 +336,10 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
                                       other-state cell on their lower-dimension lines at which the tile takes the
                                       lower-envelope path instead of the windowed search (0 = 50);
                                       1 = windowed search only, 2 = envelope only */
+#define DOL_TUNE_OCCLUSION    11   /* occlusion sweeps, by row length: 0 = block wavefront (3D blocks of 32 x 16
+                                      columns x 32 slices, 64 from 256 slices on), 1 = one CTA per plane (rows
+                                      up to 4096 cells), 2..999 = 3D blocks of that many slices, plus 1000 =
+                                      blocks of 32 x 32 columns */
 DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream);
 DOL_API int        dol_tune_get(int kind, int w);
 DOL_API void       dol_tune_set(int kind, int w, int value);

@@ -757,6 +757,9 @@ def run_dol(args):
     for nm, t in zip(names, list(ms)[:n]):
         per.setdefault(nm, []).append(t)
     kern = {k: float(np.mean(v)) for k, v in per.items()}
+    # kernels of one step: one per profiled scope, two in each "_fix" scope
+    # (the far cells and the listed fix tiles of a chunked line pass)
+    launches_per_step = sum(2 if k.endswith("_fix") else 1 for k in kern)
 
     clocks = ClockSampler(local)
     if pg:
@@ -836,7 +839,7 @@ def run_dol(args):
         "vs_baseline": None, "dtype": "u32 (exact integer EDT) -> f32", "data": "synthetic",
         "config": bench_config(ws),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "configs": configs,
     }
     print(json.dumps(line), flush=True)

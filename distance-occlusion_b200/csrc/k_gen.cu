@@ -78,7 +78,7 @@ static cudaEvent_t prof_event()
 ProfScope::ProfScope(const char* name, cudaStream_t st) : st_(st)
 {
     std::lock_guard<std::mutex> lock(g_prof_mu);
-    if (!g_prof_on) return;
+    if (!g_prof_on || !name) return;   // an unnamed scope is not profiled
     ProfEntry e{name, prof_event(), prof_event()};
     cudaEventRecord(e.a, st);
     g_prof.push_back(e);

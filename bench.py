@@ -757,9 +757,7 @@ def run_dol(args):
     for nm, t in zip(names, list(ms)[:n]):
         per.setdefault(nm, []).append(t)
     kern = {k: float(np.mean(v)) for k, v in per.items()}
-    # kernels of one step: one per profiled scope, two in each "_fix" scope
-    # (the far cells and the listed fix tiles of a chunked line pass)
-    launches_per_step = sum(2 if k.endswith("_fix") else 1 for k in kern)
+    launches_per_step = len(kern)   # kernels of one step: one per profiled scope
 
     clocks = ClockSampler(local)
     if pg:

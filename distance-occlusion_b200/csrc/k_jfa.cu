@@ -20,19 +20,28 @@ __global__ void __launch_bounds__(512) k_jfa2(const uint32_t* __restrict__ in, u
     const int o = cw * s;
     auto at = [&](int xx, int yy) { return unpack2(__ldg(in + (long long)yy * w + xx)); };
     C2 best = at(x, y);
+    int32_t bl = len(best);   // the incumbent's squared length, kept between candidates
+    // closer(): a candidate wins only when strictly shorter
+    auto consider = [&](C2 cand) {
+        const int32_t cl = len(cand);
+        if (bl > cl) {
+            best = cand;
+            bl = cl;
+        }
+    };
     // candidate order of :794-868
     if (x - s >= 0) {
-        best = closer(best, add(at(x - s, y), -o, 0));
-        if (y - s >= 0) best = closer(best, add(at(x - s, y - s), -o, -o));
-        if (y + s < h) best = closer(best, add(at(x - s, y + s), -o, +o));
+        consider(add(at(x - s, y), -o, 0));
+        if (y - s >= 0) consider(add(at(x - s, y - s), -o, -o));
+        if (y + s < h) consider(add(at(x - s, y + s), -o, +o));
     }
     if (x + s < w) {
-        best = closer(best, add(at(x + s, y), +o, 0));
-        if (y - s >= 0) best = closer(best, add(at(x + s, y - s), +o, -o));
-        if (y + s < h) best = closer(best, add(at(x + s, y + s), +o, +o));
+        consider(add(at(x + s, y), +o, 0));
+        if (y - s >= 0) consider(add(at(x + s, y - s), +o, -o));
+        if (y + s < h) consider(add(at(x + s, y + s), +o, +o));
     }
-    if (y - s >= 0) best = closer(best, add(at(x, y - s), 0, -o));
-    if (y + s < h) best = closer(best, add(at(x, y + s), 0, +o));
+    if (y - s >= 0) consider(add(at(x, y - s), 0, -o));
+    if (y + s < h) consider(add(at(x, y + s), 0, +o));
     out[(long long)y * w + x] = pack2(best);
 }
 
@@ -75,18 +84,35 @@ __global__ void __launch_bounds__(512) k_jfa3(const void* __restrict__ in, void*
         return kWideIn ? load3w(static_cast<const uint2*>(in), i) : load3(static_cast<const int16_t*>(in), i);
     };
     C3 best = ld(idx);
+    int32_t bl = len(best);   // the incumbent's squared length, kept between candidates
     // all offsets in {-s, 0, +s}^3 that stay inside, z outermost, x innermost,
-    // skipping neighbours still at max (:2419-2438)
-    const int z0 = z - s >= 0 ? -s : 0, z1 = z + s < d ? s : 0;
-    const int y0 = y - s >= 0 ? -s : 0, y1 = y + s < h ? s : 0;
-    const int x0 = x - s >= 0 ? -s : 0, x1 = x + s < w ? s : 0;
-    for (int kz = z0; kz <= z1; kz += s)
-        for (int ky = y0; ky <= y1; ky += s)
-            for (int kx = x0; kx <= x1; kx += s) {
-                C3 c = ld(idx + kz * plane + (long long)ky * w + kx);
+    // skipping neighbours still at max (:2419-2438); a candidate wins only
+    // when strictly shorter (closer())
+    // (unrolled over the 27 offsets; an offset leaving the field is skipped)
+    const bool zlo = z - s >= 0, zhi = z + s < d, ylo = y - s >= 0, yhi = y + s < h, xlo = x - s >= 0,
+               xhi = x + s < w;
+    const long long oz = (long long)s * plane, oy = (long long)s * w;
+#pragma unroll
+    for (int iz = -1; iz <= 1; iz++) {
+        const bool vz = iz == 0 || (iz < 0 ? zlo : zhi);
+#pragma unroll
+        for (int iy = -1; iy <= 1; iy++) {
+            const bool vy = iy == 0 || (iy < 0 ? ylo : yhi);
+#pragma unroll
+            for (int ix = -1; ix <= 1; ix++) {
+                const bool vx = ix == 0 || (ix < 0 ? xlo : xhi);
+                if (!(vz && vy && vx)) continue;
+                const C3 c = ld(idx + iz * oz + iy * oy + ix * s);
                 if (c.x == kMax3) continue;
-                best = closer(best, add(c, cw * kx, cw * ky, cw * kz));
+                const C3 cand = add(c, cw * s * ix, cw * s * iy, cw * s * iz);
+                const int32_t cl = len(cand);
+                if (bl > cl) {
+                    best = cand;
+                    bl = cl;
+                }
             }
+        }
+    }
     if (kWideOut)
         store3w(static_cast<uint2*>(out), idx, best);
     else

@@ -379,6 +379,99 @@ __global__ void __launch_bounds__(256) k_fastsweep3(int16_t* __restrict__ dl, in
     }
 }
 
+// Slice pipeline (the default): a CTA claims a slice kk (in sweep order,
+// from an atomic counter) and walks its rows jj = 1 .. H in order, so the
+// row before (y - dy, same slice) is the CTA's own previous result, kept in
+// registers; only the slice before (z - dz, same row) comes from another
+// CTA, through its per-row flag.  Along y a step costs one row's work, along
+// z one row's work plus the hand-over (the producer's fence and flag, the
+// poll, the load), where the anti-diagonal wavefront above pays the
+// hand-over on every step (256^3 shapes: 13.9 against 15.2 ms).  A slice is
+// claimed only by a running CTA and waits only on the slice claimed before
+// it, so the earliest unfinished slice always proceeds.  A row's own cells
+// are written by no other CTA of the sweep, so they are loaded before the
+// wait (loading the next row's during the hand-over measured 3 % slower).
+template <int S>
+__global__ void __launch_bounds__(256) k_fastsweep3_slices(int16_t* __restrict__ dl, int w, int h, int d, int cw,
+                                                           int sweep, int* __restrict__ flags,
+                                                           int* __restrict__ counter, int* __restrict__ err,
+                                                           int epoch, int wait_epoch, unsigned wait_limit)
+{
+    __shared__ ScanShared<C3> sh;
+    __shared__ int s_slice;
+    const int t = threadIdx.x;
+    const int nseg = (w + S - 1) / S;
+    const bool active = t < nseg;
+    const int n = active ? min(S, w - t * S) : 0;
+    const long long x0 = (long long)t * S;
+    const long long plane = (long long)w * h;
+    const int dx = (sweep & 1) ? -1 : 1, dy = (sweep & 2) ? -1 : 1, dz = (sweep & 4) ? -1 : 1;
+    const int oy = -cw * dy, oz = -cw * dz;
+    const int yb = dy > 0 ? 0 : h - 1, zb = dz > 0 ? 0 : d - 1;
+    const int H = h - 1, Dd = d - 1;
+    const int pred = t - dx;
+    const bool has_pred = active && pred >= 0 && pred < nseg;
+    C3 C[S], Zp[S], Yp[S], V[S], R[S], D[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) C[s] = Zp[s] = Yp[s] = V[s] = R[s] = D[s] = C3{0, 0, 0};
+
+    for (;;) {
+        if (t == 0) s_slice = atomicAdd(counter, 1) + 1;
+        __syncthreads();
+        const int kk = s_slice;
+        __syncthreads();
+        if (kk > Dd) break;
+        const int z = zb + kk * dz, zprev = z - dz;
+        // the slice's first row is not updated by the sweep (:2208, :2214 start at 1)
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            if (s < n) Yp[s] = cell_load_cg(dl, z * plane + (long long)yb * w + x0 + s);
+        for (int jj = 1; jj <= H; jj++) {
+            const int y = yb + jj * dy;
+            const long long rb = z * plane + (long long)y * w + x0;
+#pragma unroll
+            for (int s = 0; s < S; s++)
+                if (s < n) C[s] = cell_load_cg(dl, rb + s);
+            if (kk > 1 && t == 0) {
+                // wait (bounded) until the slice before has done this row
+                // (wait_epoch is epoch except under a test hook that makes it unreachable)
+                const int* fb = flags + (long long)zprev * h + y;
+                for (unsigned it = 0;; it++) {
+                    if (*((volatile const int*)fb) >= wait_epoch) break;
+                    if (it >= wait_limit) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+            }
+            __syncthreads();
+            const long long zb_ = (long long)zprev * plane + (long long)y * w + x0;
+#pragma unroll
+            for (int s = 0; s < S; s++)
+                if (s < n) {
+                    Zp[s] = cell_load_cg(dl, zb_ + s);
+                    V[s] = closer(closer(C[s], add(Zp[s], 0, 0, oz)), add(Yp[s], 0, oy, 0));
+                }
+            if (active) sh.guess[0][t] = dx > 0 ? seg_edge<C3, S, +1>(V, n) : seg_edge<C3, S, -1>(V, n);
+            __syncthreads();
+            const C3 in0 = has_pred ? sh.guess[0][pred] : V[0];
+            auto nopost = [](const C3 (&)[S]) {};
+            if (dx > 0)
+                row_pass<C3, S, false, +1>(R, V, t, nseg, n, cw, sh, D, in0, nopost);
+            else
+                row_pass<C3, S, false, -1>(R, V, t, nseg, n, cw, sh, D, in0, nopost);
+            store_row<C3, S>(dl, rb, R, n);
+#pragma unroll
+            for (int s = 0; s < S; s++) Yp[s] = R[s];   // the next row's y neighbour
+            __threadfence();
+            __syncthreads();
+            if (t == 0) atomicExch(flags + (long long)z * h + y, epoch);
+        }
+    }
+}
+
 // ------------------------------------------------------- single-warp engines ----
 // Rows of at most 32*S cells: one warp per image (or volume), every exchange a
 // shuffle, no shared memory and no CTA barrier (row_pass_warp).  Same steps
@@ -710,6 +803,8 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
     // per SM along the wavefront; 256^3 shapes: 15.1 ms at 128 threads, 22.0
     // at 256), else at most 256
     int s = tune_get(kTuneFs3, w);
+    const bool wavefront = s < 0;   // negative tuned values: the anti-diagonal wavefront with -s cells per thread
+    if (wavefront) s = -s;
     if (!((s == 1 || s == 2 || s == 4 || s == 8) && (w + s - 1) / s <= 256)) {
         s = pick_s(w, 128);
         if (!s) s = pick_s(w, 256);
@@ -719,6 +814,19 @@ void launch_fastsweep_3d(void* deltas, int w, int h, int d, int cw, void* ws, in
     ProfScope ps("fastsweep_3d", st);
 #define DOL_FS3_CASE(SV)                                                                                     \
     case SV: {                                                                                               \
+        if (!wavefront) {                                                                                    \
+            int per_sm = 0;                                                                                  \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fastsweep3_slices<SV>, T, 0);           \
+            if (per_sm < 1) per_sm = 1;                                                                      \
+            long long grid = (long long)per_sm * g_num_sms;                                                  \
+            if (grid > Dd) grid = Dd;                                                                        \
+            for (int sw = 0; sw < 8; sw++)                                                                   \
+                k_fastsweep3_slices<SV><<<(int)grid, T, 0, st>>>(static_cast<int16_t*>(deltas), w, h, d, cw,  \
+                                                                 sw, flags, counters + sw, err, sw + 1,       \
+                                                                 sw == hooks.stall_sweep ? INT_MAX : sw + 1,  \
+                                                                 hooks.limit);                                \
+            break;                                                                                           \
+        }                                                                                                    \
         int per_sm = 0;                                                                                      \
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fastsweep3<SV>, T, 0);                      \
         if (per_sm < 1) per_sm = 1;                                                                          \

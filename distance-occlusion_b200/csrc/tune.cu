@@ -79,10 +79,12 @@ static std::vector<int> candidates(int kind, int w)
             if (w <= (kind == kTuneDan3 ? 256 : 512)) c.push_back(32);
             return c;
         }
-        case kTuneFs3: {
+        case kTuneFs3: {   // the slice pipeline, then the anti-diagonal wavefront (negative)
             std::vector<int> c;
             for (int s : {1, 2, 4, 8})
                 if ((w + s - 1) / s <= 256) c.push_back(s);
+            for (int s : {1, 2, 4, 8})
+                if ((w + s - 1) / s <= 256) c.push_back(-s);
             return c;
         }
         case kTuneJfa2:
@@ -177,8 +179,11 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     int tw = w, th = h, td = vol ? d : 1;
     if (kind == kTuneFs2) th = h < 256 ? h : 256;
     if (kind == kTuneFs3) {
+        // both engines are bound by their dependency chains (rows + slices
+        // long) and the slice pipeline by its number of slices: keep enough
+        // of both for the comparison to hold at the caller's size
         th = h < 64 ? h : 64;
-        td = d < 8 ? d : 8;
+        td = d < 64 ? d : 64;
     }
     if (kind == kTuneDan3) td = d < 32 ? d : 32;   // whole slices: the block schedule's row blocks
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);

@@ -324,7 +324,8 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_DANIELSSON_2D 0   /* CTA engine with 1, 2, 4, 8 cells per thread; 32 = single-warp engine */
 #define DOL_TUNE_DANIELSSON_3D 1
 #define DOL_TUNE_FASTSWEEP_2D  2
-#define DOL_TUNE_FASTSWEEP_3D  3
+#define DOL_TUNE_FASTSWEEP_3D  3   /* cells per thread 1, 2, 4, 8: the slice pipeline (one CTA per slice in turn);
+                                      -1, -2, -4, -8: the anti-diagonal wavefront of rows */
 #define DOL_TUNE_JUMPFLOOD_2D  4   /* rows per CTA: 2, 4, 8, 16 */
 #define DOL_TUNE_JUMPFLOOD_3D  5
 #define DOL_TUNE_BATCH         6   /* cells per thread: 4 (256 threads) or 8 (128 threads) */

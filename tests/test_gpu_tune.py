@@ -20,7 +20,7 @@ def _mask(O, dims, p, seed):
     (DAN2, "danielsson", (300, 40), [1, 2, 4, 8, 32]),
     (FS2, "fastsweep", (300, 40), [1, 2, 4, 8, 32]),
     (DAN3, "danielsson", (70, 12, 9), [1, 2, 4, 8, 32]),
-    (FS3, "fastsweep", (70, 12, 9), [1, 2, 4, 8]),
+    (FS3, "fastsweep", (70, 12, 9), [1, 2, 4, 8, -1, -2, -4, -8]),
     (JFA2, "jumpflood", (300, 40), [2, 4, 8, 16]),
     (JFA3, "jumpflood", (70, 12, 9), [2, 4, 8, 16]),
 ])

@@ -66,3 +66,23 @@ def test_calls_fail_cleanly_without_device_memory(dol):
     else:
         st = dol.lib().dol_init_border_2d(C.c_int(32), C.c_int(2), None, None, None)
         assert st in (dol.ERR_CUDA, dol.ERR_INVALID_ARG)
+
+
+def test_tuning_table_round_trip(dol):
+    """dol_tune_set / dol_tune_get keep a value per family and width bucket
+    (ceil(log2(w))), negative values included (DOL_TUNE_FASTSWEEP_3D: the
+    anti-diagonal wavefront), and 0 restores the built-in heuristic."""
+    L = dol.lib()
+    FS3, OCC = 3, 11
+    try:
+        L.dol_tune_set(FS3, 256, -2)
+        assert L.dol_tune_get(FS3, 256) == -2
+        assert L.dol_tune_get(FS3, 200) == -2      # same bucket (129..256)
+        assert L.dol_tune_get(FS3, 257) == 0       # next bucket untouched
+        L.dol_tune_set(OCC, 1024, 1000)
+        assert L.dol_tune_get(OCC, 1024) == 1000
+        assert L.dol_tune_get(FS3, 256) == -2      # families are independent
+    finally:
+        L.dol_tune_set(FS3, 256, 0)
+        L.dol_tune_set(OCC, 1024, 0)
+    assert L.dol_tune_get(FS3, 256) == 0

@@ -119,6 +119,85 @@ __global__ void __launch_bounds__(512) k_jfa3(const void* __restrict__ in, void*
         store3(static_cast<int16_t*>(out), idx, best);
 }
 
+// The same pass walking z: a thread takes one column (x, y) and the cells
+// z = r + i s of one residue class r (a chunk of kJfaChunk of them), and visits
+// the slices r + j s in order, each slice's 9 neighbours of the column loaded
+// once and applied to the three cells that read them -- as offset +s for cell
+// j - 1, 0 for cell j and -s for cell j + 1.  A cell thus meets its candidates
+// in the reference's order (its own value first, then the slice below, its
+// own slice, the slice above, y then x within each), and the pass loads ~10
+// values per cell instead of 27.
+constexpr int kJfaChunk = 32;
+
+template <bool kWideIn>
+__device__ __forceinline__ C3 jfa_ld(const void* in, long long i)
+{
+    return kWideIn ? load3w(static_cast<const uint2*>(in), i) : load3(static_cast<const int16_t*>(in), i);
+}
+
+template <bool kWideIn, bool kWideOut>
+__global__ void __launch_bounds__(512) k_jfa3z(const void* __restrict__ in, void* __restrict__ out, int w, int h, int d,
+                                               int s, int cw, int nchunk)
+{
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (x >= w || y >= h) return;
+    const int r = blockIdx.z / nchunk, chunk = blockIdx.z % nchunk;
+    const int m = (d - r + s - 1) / s;   // cells r + i s < d
+    const int i0 = chunk * kJfaChunk, i1 = min(m, i0 + kJfaChunk);
+    if (i0 >= i1) return;
+    const long long plane = (long long)w * h;
+    const long long col = (long long)y * w + x;
+    const bool ylo = y - s >= 0, yhi = y + s < h, xlo = x - s >= 0, xhi = x + s < w;
+    const int o = cw * s;
+    // the three cells a slice serves: A = j - 1 (offset +s), B = j (0), C = j + 1 (-s)
+    C3 bA{0, 0, 0}, bB{0, 0, 0}, bC{0, 0, 0};
+    int32_t lA = 0, lB = 0, lC = 0;
+    auto consider = [](C3& best, int32_t& bl, const C3& cand) {
+        const int32_t cl = len(cand);
+        if (bl > cl) {   // strictly shorter (closer())
+            best = cand;
+            bl = cl;
+        }
+    };
+    for (int j = i0 - 1; j <= i1; j++) {
+        const bool hasA = j - 1 >= i0, hasB = j >= i0 && j < i1, hasC = j + 1 < i1;
+        if (hasC) {   // cell j + 1 starts from its own value
+            bC = jfa_ld<kWideIn>(in, (long long)(r + (j + 1) * s) * plane + col);
+            lC = len(bC);
+        }
+        if (j >= 0 && j < m) {   // slice r + j s exists: its 9 neighbours of the column
+            const long long base = (long long)(r + j * s) * plane + col;
+#pragma unroll
+            for (int iy = -1; iy <= 1; iy++) {
+                const bool vy = iy == 0 || (iy < 0 ? ylo : yhi);
+#pragma unroll
+                for (int ix = -1; ix <= 1; ix++) {
+                    const bool vx = ix == 0 || (ix < 0 ? xlo : xhi);
+                    if (!(vy && vx)) continue;
+                    const C3 c = jfa_ld<kWideIn>(in, base + (long long)iy * s * w + ix * s);
+                    if (c.x == kMax3) continue;
+                    const int cx = trunc16(c.x + o * ix), cy = trunc16(c.y + o * iy);
+                    if (hasC) consider(bC, lC, C3{cx, cy, trunc16(c.z - o)});
+                    if (hasB) consider(bB, lB, C3{cx, cy, c.z});
+                    if (hasA) consider(bA, lA, C3{cx, cy, trunc16(c.z + o)});
+                }
+            }
+        }
+        if (hasA) {   // cell j - 1 has seen its three slices
+            const long long idx = (long long)(r + (j - 1) * s) * plane + col;
+            if (kWideOut)
+                store3w(static_cast<uint2*>(out), idx, bA);
+            else
+                store3(static_cast<int16_t*>(out), idx, bA);
+        }
+        bA = bB;
+        lA = lB;
+        bB = bC;
+        lB = lC;
+    }
+}
+
 size_t jumpflood_workspace_bytes(int dim, int w, int h, int d)
 {
     const size_t cells = (size_t)w * h * (dim == 3 ? d : 1);
@@ -142,6 +221,8 @@ void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, in
     if (dim == 3 && d > m) m = d;
     // rows per CTA (32 x ry threads): tuned, else 8
     int ry = tune_get(dim == 2 ? kTuneJfa2 : kTuneJfa3, w);
+    const bool per_cell = dim == 3 && ry < 0;   // 3D, negative tuned values: one thread per cell (k_jfa3)
+    if (per_cell) ry = -ry;
     if (ry != 2 && ry != 4 && ry != 8 && ry != 16) ry = 8;
     // the reference's schedule: steps FloorPow2(m - 1) .. 1 ping-ponging with
     // the caller's buffer, plus one step-1 pass when the result would end in temp
@@ -172,12 +253,26 @@ void launch_jumpflood(int dim, void* deltas, void* temp, int w, int h, int d, in
         const bool first = i == 0, last = i == np - 1;
         const void* src = first ? deltas : wb[(i - 1) & 1];
         void* dst = last ? deltas : wb[i & 1];
+        const int sv = steps[i];
+        if (per_cell) {
+            if (first)
+                k_jfa3<false, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw);
+            else if (last)
+                k_jfa3<true, false><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw);
+            else
+                k_jfa3<true, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw);
+            continue;
+        }
+        // z walk: residue classes of z mod s, chunks of kJfaChunk cells along each
+        const int nres = sv < d ? sv : d;
+        const int nchunk = ((d + sv - 1) / sv + kJfaChunk - 1) / kJfaChunk;
+        const dim3 gz((w + 31) / 32, (h + ry - 1) / ry, (unsigned)(nres * nchunk));
         if (first)
-            k_jfa3<false, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+            k_jfa3z<false, true><<<gz, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw, nchunk);
         else if (last)
-            k_jfa3<true, false><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+            k_jfa3z<true, false><<<gz, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw, nchunk);
         else
-            k_jfa3<true, true><<<grid, 32 * ry, 0, st>>>(src, dst, w, h, d, steps[i], cw);
+            k_jfa3z<true, true><<<gz, 32 * ry, 0, st>>>(src, dst, w, h, d, sv, cw, nchunk);
     }
 }
 

@@ -87,8 +87,8 @@ static std::vector<int> candidates(int kind, int w)
                 if ((w + s - 1) / s <= 256) c.push_back(-s);
             return c;
         }
-        case kTuneJfa2:
-        case kTuneJfa3: return {2, 4, 8, 16};
+        case kTuneJfa2: return {2, 4, 8, 16};
+        case kTuneJfa3: return {2, 4, 8, 16, -2, -4, -8, -16};   // z walk, then one thread per cell
         case kTuneBatch: return {4, 8};
         case kTuneEdt: return {256, 512};
         case kTuneDanRows: return {4, 8, 16, 32, kDanSerial};
@@ -180,10 +180,16 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     if (kind == kTuneFs2) th = h < 256 ? h : 256;
     if (kind == kTuneFs3) {
         // both engines are bound by their dependency chains (rows + slices
-        // long) and the slice pipeline by its number of slices: keep enough
-        // of both for the comparison to hold at the caller's size
-        th = h < 64 ? h : 64;
-        td = d < 64 ? d : 64;
+        // long) and the slice pipeline by its number of slices, so the ranking
+        // changes with the shape (256 x 64 x 64 ranks 1 cell per thread first,
+        // 256^3 2 cells): the caller's shape up to 2^25 cells, beyond that rows
+        // and slices halved in turn
+        while ((long long)tw * th * td > (1LL << 25) && (th > 64 || td > 64)) {
+            if (th >= td)
+                th = (th + 1) / 2;
+            else
+                td = (td + 1) / 2;
+        }
     }
     if (kind == kTuneDan3) td = d < 32 ? d : 32;   // whole slices: the block schedule's row blocks
     if (kind == kTuneJfa2 && (long long)tw * th > (1LL << 22)) th = (int)((1LL << 22) / tw > 0 ? (1LL << 22) / tw : 1);

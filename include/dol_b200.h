@@ -327,7 +327,7 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_FASTSWEEP_3D  3   /* cells per thread 1, 2, 4, 8: the slice pipeline (one CTA per slice in turn);
                                       -1, -2, -4, -8: the anti-diagonal wavefront of rows */
 #define DOL_TUNE_JUMPFLOOD_2D  4   /* rows per CTA: 2, 4, 8, 16 */
-#define DOL_TUNE_JUMPFLOOD_3D  5
+#define DOL_TUNE_JUMPFLOOD_3D  5   /* rows per CTA 2, 4, 8, 16 of the z walk; negative: one thread per cell */
 #define DOL_TUNE_BATCH         6   /* cells per thread: 4 (256 threads) or 8 (128 threads) */
 #define DOL_TUNE_EDT           7   /* threads per CTA of the line passes: 256 or 512 */
 #define DOL_TUNE_DANIELSSON_ROWS 8 /* Danielsson block schedule: rows per block (1..4096);

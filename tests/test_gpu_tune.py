@@ -22,7 +22,8 @@ def _mask(O, dims, p, seed):
     (DAN3, "danielsson", (70, 12, 9), [1, 2, 4, 8, 32]),
     (FS3, "fastsweep", (70, 12, 9), [1, 2, 4, 8, -1, -2, -4, -8]),
     (JFA2, "jumpflood", (300, 40), [2, 4, 8, 16]),
-    (JFA3, "jumpflood", (70, 12, 9), [2, 4, 8, 16]),
+    (JFA3, "jumpflood", (70, 12, 9), [2, 4, 8, 16, -2, -4, -8, -16]),
+    (JFA3, "jumpflood", (40, 33, 70), [8, -8]),
 ])
 def test_every_candidate_gives_the_same_deltas(dol, O, cuda, kind, method, dims, values):
     torch = cuda
@@ -57,7 +58,8 @@ def test_edt_threads_do_not_change_results(dol, O, cuda):
 
 
 @pytest.mark.parametrize("kind,dims,values", [
-    (DAN2, (512, 512, 1), {1, 2, 4, 8, 32}), (FS3, (128, 64, 32), {1, 2, 4}), (JFA3, (128, 128, 128), {2, 4, 8, 16}),
+    (DAN2, (512, 512, 1), {1, 2, 4, 8, 32}), (FS3, (128, 64, 32), {1, 2, 4, -1, -2, -4}),
+    (JFA3, (128, 128, 128), {2, 4, 8, 16, -2, -4, -8, -16}),
     (EDT, (256, 256, 256), {256, 512}), (BATCH, (1024, 1, 1), {4, 8})])
 def test_autotune_picks_a_candidate(dol, cuda, kind, dims, values):
     L = dol.lib()

@@ -338,10 +338,8 @@ def measure_configs(dol, torch, cpu=True, big=True, only=None):
     want = (lambda key: only is None or key in only)
     # launch configurations chosen by the library's autotuner (untimed)
     tuned = {}
-    # (FastSweep 3D keeps its default: the tuner's problem of scattered seeds
-    # ranks 1 cell per thread first, the 256^3 shapes volume 2 cells, the default)
     for name, kind, shape in (("danielsson_2d", 0, (1024, 1024, 1)), ("danielsson_3d", 1, (256, 256, 256)),
-                              ("jumpflood_3d", 5, (256, 256, 256)),
+                              ("fastsweep_3d", 3, (256, 256, 256)), ("jumpflood_3d", 5, (256, 256, 256)),
                               ("batch", 6, (1024, 1, 1)), ("edt", 7, (1024, 1024, 1024))):
         if L.dol_autotune(kind, *shape, sp) == 0:
             tuned[name] = L.dol_tune_get(kind, shape[0])

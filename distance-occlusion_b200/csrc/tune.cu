@@ -11,6 +11,7 @@
 // keeps the fastest; dol_tune_set pins a value by hand.
 #include <float.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -205,7 +206,8 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
     const long long cells = (long long)tw * th * td;
     const size_t mwords = (size_t)((tw + 31) / 32) * th * td;
 
-    // seeds: a sparse LCG scatter (delta methods) or value noise (EDT), on the host
+    // seeds: a sparse LCG scatter (delta methods), solids (FastSweep 3D) or
+    // value noise (EDT)
     std::vector<uint32_t> hm(mwords, 0u);
     uint32_t seed = 77;
     const long long nseeds = cells / 64 + 1;
@@ -234,9 +236,16 @@ DOL_API dol_status dol_autotune(int kind, int w, int h, int d, void* stream)
             if (p) cudaFreeAsync(p, st);
         return (dol_status)set_error(DOL_ERR_NO_MEMORY, "autotune scratch allocation failed");
     }
-    if (kind == kTuneEdt)
+    if (kind == kTuneEdt) {
         dol_gen_value_noise_3d(tw, th, td, 16, 3u, static_cast<uint32_t*>(dm), st);
-    else
+    } else if (kind == kTuneFs3) {
+        // FastSweep 3D ranks its candidates differently on a scatter of single
+        // seeds (1 cell per thread first) and on solids (2 cells on the 256^3
+        // volume of boxes and spheres): tune it on solids, sized to the volume
+        const int m = std::min(tw, std::min(th, td));
+        dol_gen_shapes_3d(tw, th, td, 32, 32, std::max(1, 4 * m / 256), std::max(2, 40 * m / 256), 5u,
+                          static_cast<uint32_t*>(dm), st);
+    } else
         cudaMemcpyAsync(dm, hm.data(), mwords * 4, cudaMemcpyHostToDevice, st);
     int* err = nullptr;
     cudaMallocAsync((void**)&err, sizeof(int), st);

@@ -61,24 +61,71 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    queries (read only) from a thread every 2 ms, else nvidia-smi, whose
+    samples count from the first one after its start-up."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+            ("sw_power_cap", 0x4))
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.nvml = None
+        self.n0 = 0
+
+    def _start_nvml(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            try:
+                import torch
+                u = str(torch.cuda.get_device_properties(self.idx).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            reasons = (getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or
+                       pynvml.nvmlDeviceGetCurrentClocksThrottleReasons)
+            mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            reasons(h)
+        except Exception:
+            return False
+        self.nvml = pynvml
+        self.stop_ev = threading.Event()
+
+        def loop():
+            while not self.stop_ev.is_set():
+                try:
+                    self.samples.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)), mx,
+                                         int(reasons(h))))
+                except Exception:
+                    break
+                self.stop_ev.wait(0.002)
+
+        self.t = threading.Thread(target=loop, daemon=True)
+        self.t.start()
+        return True
 
     def start(self):
+        if self._start_nvml():
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "10"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.005)
+            self.n0 = len(self.lines)
         except Exception:
             self.proc = None
 
@@ -87,6 +134,18 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            sm = [x[0] for x in self.samples]
+            reasons = sorted({n for _, _, r in self.samples for n, bit in self.BITS if r & bit})
+            return {"sm_mhz": float(np.median(sm)) if sm else None,
+                    "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -95,8 +154,9 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        names = [n for n, _ in self.BITS]
+        lines = self.lines[self.n0:] or self.lines[-1:]   # none inside a short region: the next one
+        for ln in lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -109,7 +169,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def max_over_ranks(x, pg, device="cuda"):

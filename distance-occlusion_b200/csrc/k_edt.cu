@@ -435,14 +435,25 @@ __device__ __forceinline__ uint32_t far_side(uint32_t best, int q, int n, int k,
     return best;
 }
 
+// Blocks of the pruned search (uint32 tiles): kPruneB cells, their minima kept
+// per (state, column)
+constexpr int kPruneB = 16;
+// a uint32 tile takes the pruned search when far_pct percent of its sampled
+// cells lie at least kFarDist cells from the other state in their plane (1024^3
+// z passes: 2000 random points, ~90 % of the cells, 14.2 -> 11.7 ms; 20000
+// points, ~37 %, stay on the windowed search, 8.2 against 9.5 ms pruned)
+constexpr uint32_t kFarDist = 128;
+
 // the two split line arrays with their sentinel rows, then the envelope
-// path's hull words (two per column per 32-cell segment)
+// path's hull words (two per column per 32-cell segment), then (uint32
+// tiles) the pruned search's block minima (two per column per block)
 template <typename TIn, int TX>
 static size_t tma_tile_bytes(int n)
 {
     constexpr int SB = 32;
     return 2 * (size_t)(((n + 255) / 256) * 256 + 2 * kPadRows) * TX * sizeof(TIn) +
-           2 * (size_t)TX * ((n + SB - 1) / SB) * sizeof(uint32_t);
+           2 * (size_t)TX * ((n + SB - 1) / SB) * sizeof(uint32_t) +
+           (sizeof(TIn) == 4 ? 2 * (size_t)TX * ((n + kPruneB - 1) / kPruneB) * sizeof(uint32_t) : 0);
 }
 
 // One 32-bit word of a staged tile split by state: its cells (two uint16 or
@@ -508,10 +519,88 @@ __device__ __noinline__ void edt_tile_envelope(const TIn* F0, TIn* F1, int rows,
     }
 }
 
+// Pruned search (uint32 tiles whose cells mostly lie far from the other
+// state in their plane: the z pass of a sparse volume, whose cells see a
+// candidate in most planes but far away).  The line is cut into blocks of
+// kPruneB cells with each block's smallest F_s value; a cell scans its own
+// block, then visits blocks outwards on both sides, skipping a block when its
+// minimum plus the squared distance to its nearest cell is not below the best
+// value, and stops when the nearer unvisited block is at least sqrt(best)
+// away.  Every skipped candidate is bounded below by the block's bound, so the
+// result is the exact minimum over the line, the windowed search's.
+template <typename TIn, bool kFinal, int TX, int kMode>
+__device__ __noinline__ void edt_tile_pruned(const TIn* F0, const TIn* F1, int rows, int n, int w, int x0, int outer,
+                                             void* out, long long stride, long long outer_stride, int form)
+{
+    if (sizeof(TIn) != 4) return;   // uint32 tiles only (the launcher never asks otherwise)
+    constexpr int B = kPruneB;
+    const int nseg = (n + 31) / 32, nb = (n + B - 1) / B;
+    uint32_t* MB = reinterpret_cast<uint32_t*>(const_cast<TIn*>(F1) + (rows + 2 * kPadRows) * TX - kPadRows * TX) +
+                   2 * TX * nseg;   // [state][block][column]
+    // block minima; the rows of a block are read rotated by the block so that
+    // a warp's lanes (8 columns x 4 blocks) hit different banks
+    for (int jb = threadIdx.x; jb < 2 * nb * TX; jb += blockDim.x) {
+        const int col = jb % TX, j = (jb / TX) % nb, st = jb / (TX * nb);
+        const TIn* A = (st ? F1 : F0) + (size_t)j * B * TX + col;
+        uint32_t m = 0xFFFFFFFFu;
+        for (int i = 0; i < B; i++) m = min(m, (uint32_t)A[((i + j) & (B - 1)) * TX]);
+        MB[jb] = m;
+    }
+    __syncthreads();
+    constexpr int kGroups = TX / 8;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, wi = threadIdx.x >> 5;
+    const int col = (wi % kGroups) * 8 + (lane & 7), sub = lane >> 3;
+    const int qstep = 8 * (nw / kGroups);
+    const int x = x0 + col;
+    if (x >= w) return;
+    const long long base = kMode == 1 ? ((long long)(x >> 3) * outer_stride + outer) * 8 + (x & 7)
+                                      : (long long)outer * outer_stride + x;
+    const uint32_t kNone = kInf32;
+    for (int qa = 8 * (wi / kGroups) + sub; qa < n; qa += qstep) {
+        for (int h = 0; h < 2; h++) {   // the lane's two cells, 4 positions apart (the windowed path's cells)
+            const int q = qa + 4 * h;
+            if (q >= n) break;
+            const uint32_t c0 = F0[q * TX + col], c1 = F1[q * TX + col];
+            const uint32_t s = c1 != 0;
+            const TIn* A = (s ? F1 : F0) + col;
+            const uint32_t* M = MB + (size_t)s * nb * TX + col;
+            uint32_t best = c0 | c1;
+            const int j0 = q / B;
+            {   // the own block: distances j0 * B - q .. j0 * B + B - 1 - q
+                int dd = j0 * B - q;
+                const TIn* pa = A + (size_t)j0 * B * TX;
+#pragma unroll
+                for (int i = 0; i < B; i++, dd++) best = __viaddmin_u32((uint32_t)pa[i * TX], (uint32_t)(dd * dd), best);
+            }
+            for (int r = 1;; r++) {
+                const int jl = j0 - r, jr = j0 + r;
+                const uint32_t dl = (uint32_t)(q - jl * B - (B - 1)), dr = (uint32_t)(jr * B - q);
+                const uint32_t dl2 = dl * dl, dr2 = dr * dr;
+                const bool okl = jl >= 0 && dl2 < best, okr = jr < nb && dr2 < best;
+                if (!okl && !okr) break;
+                if (okl && M[(size_t)jl * TX] + dl2 < best) {   // leftwards from the block's last cell
+                    const TIn* pa = A + ((size_t)jl * B + B - 1) * TX;
+                    uint32_t d = dl;
+#pragma unroll
+                    for (int i = 0; i < B; i++, d++) best = __viaddmin_u32((uint32_t)pa[-i * TX], d * d, best);
+                }
+                if (okr && M[(size_t)jr * TX] + dr2 < best) {
+                    const TIn* pa = A + (size_t)jr * B * TX;
+                    uint32_t d = dr;
+#pragma unroll
+                    for (int i = 0; i < B; i++, d++) best = __viaddmin_u32((uint32_t)pa[i * TX], d * d, best);
+                }
+            }
+            put_walk_value<kFinal>(out, base + (long long)q * stride, s, best, best >= kNone, form);
+        }
+    }
+}
+
 template <typename TIn, bool kFinal, int TX, int kMode>
 __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CUtensorMap map, void* __restrict__ out,
                                                       int w, int n, long long stride, long long outer_stride,
-                                                      int along_z, int form, int* err, int outer0, uint32_t hull_pct)
+                                                      int along_z, int form, int* err, int outer0, uint32_t hull_pct,
+                                                      uint32_t far_pct)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nbox = (n + 255) >> 8;
@@ -578,11 +667,15 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
         split_word<TIn>(x.w, sw, &a.w, &b.w);
         V0[i] = a;
         V1[i] = b;
-        if (hull_pct <= 100u) {   // uniform; skipped when the envelope path is off
-            if (sizeof(TIn) == 2)
+        if (hull_pct <= 100u || far_pct <= 100u) {   // uniform; skipped when both other paths are off
+            if (sizeof(TIn) == 2) {
                 score += __vcmpeq2(x.x & sw, sw) & 0x00010001u;   // one per "none" half, summed per half
-            else
-                score += (x.x & sw) == sw;
+            } else {
+                // low half: "none" cells; high half: cells at least kFarDist
+                // from the other state in their plane ("none" included)
+                const uint32_t v = x.x & sw;
+                score += (uint32_t)(v == sw) + ((uint32_t)(v >= kFarDist * kFarDist) << 16);
+            }
         }
     }
     for (int i = n * kVecRow + threadIdx.x; i < (rows + kPadRows) * kVecRow; i += blockDim.x) {
@@ -598,10 +691,15 @@ __global__ void __launch_bounds__(512) k_edt_line_tma(const __grid_constant__ CU
     if ((threadIdx.x & 31) == 0 && score) atomicAdd(&s_score, score);
     __syncthreads();
     const long long sampled = (long long)n * min(TX, w - x0) / 4;
-    const bool use_hull = hull_pct <= 100u && 100LL * s_score >= (long long)hull_pct * sampled;
+    const uint32_t n_none = sizeof(TIn) == 2 ? s_score : (s_score & 0xFFFFu), n_far = s_score >> 16;
+    const bool use_hull = hull_pct <= 100u && 100LL * n_none >= (long long)hull_pct * sampled;
 
     if (use_hull) {
         edt_tile_envelope<TIn, kFinal, TX, kMode>(F0, F1, rows, n, w, x0, outer, out, stride, outer_stride, form);
+        return;
+    }
+    if (sizeof(TIn) == 4 && far_pct <= 100u && 100LL * n_far >= (long long)far_pct * sampled) {
+        edt_tile_pruned<TIn, kFinal, TX, kMode>(F0, F1, rows, n, w, x0, outer, out, stride, outer_stride, form);
         return;
     }
 
@@ -743,15 +841,27 @@ static bool blocked_layout_ok(const uint16_t* vx, const uint32_t* ey, int w, int
 // Share of "none" cells (percent) at which a line-pass tile takes the
 // envelope path; above 100: never.  The tuned value (DOL_TUNE_EDT_HULL, by
 // line length): 1 = windowed search only, 2 = envelope only, 3..100 = that
-// percentage; 0 = 50 (the tiles of sparse and empty volumes; dense fields,
-// and fields whose far cells still see a candidate, keep the windowed search,
-// which is faster there).
+// percentage, 101 / 102 = no envelope path / the default share without the
+// pruned search; 0 = 50 (the tiles of sparse and empty volumes; dense fields
+// keep the windowed search, and uint32 tiles whose far cells still see a
+// candidate take the pruned search, both faster there).
 static uint32_t edt_hull_share(int n)
 {
     const int v = tune_get(kTuneEdtHull, n);
-    if (v == 1) return 0xFFFFFFFFu;
+    if (v == 1 || v == 101) return 0xFFFFFFFFu;
     if (v == 2) return 0u;
     return v >= 3 && v <= 100 ? (uint32_t)v : 50u;
+}
+
+// Share of far cells (percent) at which a uint32 tile that does not take the
+// envelope path takes the pruned search; above 100: never.  DOL_TUNE_EDT_HULL
+// 101 sends every such tile there, 102 keeps the windowed search.
+static uint32_t edt_far_share(int n)
+{
+    const int v = tune_get(kTuneEdtHull, n);
+    if (v == 101) return 0u;
+    if (v == 1 || v == 102) return 0xFFFFFFFFu;
+    return 50u;
 }
 
 // Lines along y (along_z = 0, outer index = z) or z (along_z = 1, outer = y)
@@ -773,7 +883,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
     const bool aligned = ((size_t)w * sizeof(TIn)) % 16 == 0 && ((uintptr_t)in % 16) == 0;
     const int tv = tune_get(kTuneEdt, w);
     const int threads = tv == 256 ? 256 : 512;
-    const uint32_t hthr = edt_hull_share(n);
+    const uint32_t hthr = edt_hull_share(n), fthr = edt_far_share(n);
     CUtensorMap map;
     if (mode == 1) {
         if (!line_map<TIn, TX>(&map, in, w, h, d, along_z, 0)) return;   // blocked_layout_ok encoded it already
@@ -781,7 +891,8 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         dim3 grid((w + TX - 1) / TX, (unsigned)outer);
-        kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0, hthr);
+        kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, (long long)w * d, d, along_z, form, err, outer0, hthr,
+                                                fthr);
         return;
     }
     if (mode == 2) {
@@ -795,7 +906,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         const unsigned blocks = (unsigned)(outer * (w / 8));
-        kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0, hthr);
+        kern<<<blocks, threads, tile_bytes, st>>>(map, out, w, n, plane, w, along_z, form, err, outer0, hthr, fthr);
         return;
     }
     if (aligned && tile_bytes <= 200 * 1024 && outer <= 65535) {
@@ -805,7 +916,7 @@ static void line_pass(const TIn* in, void* out, int w, int h, int d, int along_z
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             dim3 grid((w + TX - 1) / TX, (unsigned)outer);
             kern<<<grid, threads, tile_bytes, st>>>(map, out, w, n, stride, outer_stride, along_z, form, err, outer0,
-                                                    hthr);
+                                                    hthr, fthr);
             return;
         }
     }

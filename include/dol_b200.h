@@ -336,7 +336,10 @@ DOL_API dol_status dol_sites_backward(int dim, int w, int h, int d, int n_sites,
 #define DOL_TUNE_EDT_HULL     10   /* EDT line passes, by line length: the percentage of a tile's cells with no
                                       other-state cell on their lower-dimension lines at which the tile takes the
                                       lower-envelope path instead of the windowed search (0 = 50);
-                                      1 = windowed search only, 2 = envelope only */
+                                      1 = windowed search only, 2 = envelope only; z passes: tiles with half
+                                      their cells 128 or more from the other state in their plane take the
+                                      block-pruned search, 101 = for every tile not on the envelope path, 102 =
+                                      never */
 #define DOL_TUNE_OCCLUSION    11   /* occlusion sweeps, by row length: 0 = block wavefront (3D blocks of 32 x 16
                                       columns x 32 slices, 64 from 256 slices on), 1 = one CTA per plane (rows
                                       up to 4096 cells), 2..999 = 3D blocks of that many slices, plus 1000 =

@@ -54,3 +54,28 @@ def test_reference_sample_matches_whole_transform(bench, O, fraction):
     for s in range(2):
         np.testing.assert_array_equal(rs.A[s][z0:z1, :, x0:x1], rs.Y[s][:, :, x0:x1])
     assert rs.voxels * fraction == n ** 3
+
+
+def test_clock_sampler_reads_nvml_reasons(bench, monkeypatch):
+    """The timed region's clock record through NVML (a fake module here):
+    samples taken while the region runs, reason bits mapped to their names."""
+    import sys
+    import time
+    import types
+    fake = types.ModuleType("pynvml")
+    fake.NVML_CLOCK_SM = 1
+    fake.nvmlInit = lambda: None
+    fake.nvmlShutdown = lambda: None
+    fake.nvmlDeviceGetHandleByUUID = lambda u: "h"
+    fake.nvmlDeviceGetHandleByIndex = lambda i: "h"
+    fake.nvmlDeviceGetMaxClockInfo = lambda h, c: 1965
+    fake.nvmlDeviceGetClockInfo = lambda h, c: 1950
+    fake.nvmlDeviceGetCurrentClocksEventReasons = lambda h: 0x4 | 0x40
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.03)
+    rec = c.stop()
+    assert rec["source"] == "nvml" and rec["samples"] > 0
+    assert rec["sm_mhz"] == 1950.0 and rec["sm_max_mhz"] == 1965.0
+    assert rec["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]

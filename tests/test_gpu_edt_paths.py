@@ -1,9 +1,12 @@
-"""The mask EDT's two line-pass paths give the same floats as the oracle.
+"""The mask EDT's three line-pass paths give the same floats as the oracle.
 
 The y and z passes pick, per tile, the windowed search (every cell's own value
-small) or the lower-envelope path (csrc/hull.cuh; cells far from the other
-state, e.g. sparse or empty volumes).  DOL_TUNE_EDT_HULL forces either: 1 =
-windowed search only, 2 = envelope only, 0 = the automatic choice.  Every
+small), the lower-envelope path (csrc/hull.cuh; cells with no other-state
+cell on their lower-dimension lines, e.g. sparse or empty volumes) or, for
+the uint32 z pass, the block-pruned search (cells far from the other state in
+their plane).  DOL_TUNE_EDT_HULL forces them: 1 = windowed search only, 2 =
+envelope only, 101 = the pruned search for every z tile (windowed y), 102 =
+the automatic choice without the pruned search, 0 = the automatic choice.  Every
 setting must reproduce the reference's Felzenszwalb bit for bit, in all three
 output forms, on dense, sparse, empty and full inputs, for lines of one or
 several TMA boxes and both volume layouts (w a multiple of 8 or not).
@@ -61,7 +64,7 @@ DIMS = [(64, 64), (100, 37), (333, 129), (24, 20, 16), (33, 6, 5), (40, 70, 9), 
 KINDS = ["points", "empty", "full", "blocks", "0.003", "0.3"]
 
 
-@pytest.mark.parametrize("mode", [1, 2, 0])
+@pytest.mark.parametrize("mode", [1, 2, 101, 102, 0])
 @pytest.mark.parametrize("dims", DIMS)
 def test_edt_paths_match_oracle(dol, O, cuda, hull_mode, dims, mode):
     torch = cuda
